@@ -1,0 +1,186 @@
+"""ctypes front-end for the two CPU oracles (test infrastructure only).
+
+* ``PortSolver`` -- the C restatement (oracle/ns3d_oracle.c, built into
+  oracle/_build/libns3d_oracle.so).  Always available.
+* ``RefSolver``  -- the unmodified reference sources compiled in place with
+  single-rank stand-ins (oracle/_ref/libns3d_ref.so).  Available only where it
+  has been built (it needs the reference sources at build time).
+
+Both expose the same methods; arrays come back in Field3D layout
+(idx3 = (k*sy + j)*sx + i, reshaped to [sz, sy, sx]).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "_build", "libns3d_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libns3d_ref.so")
+REF_SRC_DIR = "/root/reference"
+
+_dp = C.POINTER(C.c_double)
+
+
+class OrcConfig(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("Pr", C.c_double), ("Ma", C.c_double), ("Re", C.c_double),
+                ("cfl", C.c_double), ("dt_fixed", C.c_double), ("mdcd_diss", C.c_double),
+                ("mdcd_disp", C.c_double), ("sutherland_s", C.c_double), ("Lx", C.c_double),
+                ("Ly", C.c_double), ("Lz", C.c_double), ("nx", C.c_int), ("ny", C.c_int),
+                ("nz", C.c_int), ("interpolation", C.c_int), ("riemann", C.c_int),
+                ("char_recon", C.c_int), ("bc", C.c_int * 6)]
+
+
+def build(ref: bool = True) -> None:
+    """Compile the restatement, and the reference when its sources are present."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if ref and os.path.isdir(REF_SRC_DIR):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_DIR={REF_SRC_DIR}"], check=True)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class _Base:
+    lib: C.CDLL
+
+    def _shape(self):
+        d = (C.c_int * 6)()
+        self._dims(d)
+        return list(d)
+
+    def get(self, name: str) -> np.ndarray:
+        nx, ny, nz = self.nx, self.ny, self.nz
+        sx, sy, sz = nx + 6, ny + 6, nz + 6
+        if name.startswith("flux_fx"):
+            shape = (sz, sy, sx - 1)
+        elif name.startswith("flux_fy"):
+            shape = (sz, sy - 1, sx)
+        elif name.startswith("flux_fz"):
+            shape = (sz - 1, sy, sx)
+        else:
+            shape = (sz, sy, sx)
+        out = np.empty(shape, dtype=np.float64)
+        r = self._get(name.encode(), _ptr(out), C.c_long(out.size))
+        if r < 0:
+            raise KeyError(name)
+        return out
+
+    def set(self, name: str, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        r = self._set(name.encode(), _ptr(a), C.c_long(a.size))
+        if r != 0:
+            raise KeyError(f"{name}: {r}")
+
+    def set_interior_prims(self, rho, u, v, w, p) -> None:
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, v, w, p)]
+        r = self._set_interior(*[_ptr(a) for a in arrs])
+        if r != 0:
+            raise RuntimeError("set_interior_prims failed")
+
+    def conserved(self) -> np.ndarray:
+        return np.stack([self.get(n) for n in ("rho", "rhou", "rhov", "rhow", "E")])
+
+    def rhs(self) -> np.ndarray:
+        return np.stack([self.get(n) for n in ("rhs_rho", "rhs_rhou", "rhs_rhov", "rhs_rhow", "rhs_E")])
+
+
+class PortSolver(_Base):
+    """The C restatement (oracle/ns3d_oracle.c)."""
+
+    def __init__(self, P, G):
+        if not os.path.exists(PORT_LIB):
+            build(ref=False)
+        lib = C.CDLL(PORT_LIB)
+        lib.orc_init.argtypes = [C.POINTER(OrcConfig)]
+        lib.orc_get.restype = C.c_long
+        lib.orc_get.argtypes = [C.c_char_p, _dp, C.c_long]
+        lib.orc_set.argtypes = [C.c_char_p, _dp, C.c_long]
+        lib.orc_set_interior_prims.argtypes = [_dp] * 5
+        lib.orc_rk3_step.argtypes = [C.c_double]
+        lib.orc_timestep.restype = C.c_double
+        lib.orc_total_energy.restype = C.c_double
+        lib.orc_weno5.restype = C.c_double
+        lib.orc_weno5.argtypes = [_dp]
+        lib.orc_mdcd_linear.restype = C.c_double
+        lib.orc_mdcd_linear.argtypes = [_dp, C.c_double, C.c_double]
+        lib.orc_mdcd_hybrid.restype = C.c_double
+        lib.orc_mdcd_hybrid.argtypes = [_dp, C.c_double, C.c_double]
+        lib.orc_riemann.argtypes = [C.c_int, _dp, _dp, C.c_int, C.c_double, _dp]
+        self.lib = lib
+        cfg = OrcConfig()
+        cfg.gamma, cfg.Pr, cfg.Ma, cfg.Re = P.gamma, P.Pr, P.Ma, P.Re
+        cfg.cfl, cfg.dt_fixed = P.cfl, P.dt_fixed
+        cfg.mdcd_diss, cfg.mdcd_disp, cfg.sutherland_s = P.mdcd_diss, P.mdcd_disp, P.S_ref
+        cfg.Lx, cfg.Ly, cfg.Lz = G.Lx, G.Ly, G.Lz
+        cfg.nx, cfg.ny, cfg.nz = G.global_nx, G.global_ny, G.global_nz
+        cfg.interpolation, cfg.riemann, cfg.char_recon = int(P.interpolation), int(P.riemann_solver), int(P.char_recon)
+        for i, b in enumerate(P.bcs):
+            cfg.bc[i] = int(b)
+        r = lib.orc_init(C.byref(cfg))
+        if r != 0:
+            raise ValueError(f"oracle rejected the configuration ({r})")
+        self.nx, self.ny, self.nz = G.global_nx, G.global_ny, G.global_nz
+        self._get, self._set = lib.orc_get, lib.orc_set
+        self._set_interior = lib.orc_set_interior_prims
+
+    def compute_rhs(self): self.lib.orc_compute_rhs()
+    def apply_boundary(self): self.lib.orc_apply_boundary()
+    def rk3_step(self, dt: float): self.lib.orc_rk3_step(C.c_double(dt))
+    def timestep(self) -> float: return self.lib.orc_timestep()
+    def total_energy(self) -> float: return self.lib.orc_total_energy()
+
+
+class RefSolver(_Base):
+    """The reference sources compiled in place (oracle/_ref/libns3d_ref.so)."""
+
+    def __init__(self, P, G, solver_in_text: Optional[str] = None):
+        from ns3d_wcns_b200.config import format_solver_in
+        if not ref_available():
+            raise FileNotFoundError(REF_LIB)
+        lib = C.CDLL(REF_LIB)
+        lib.ref_init_file.argtypes = [C.c_char_p, C.c_double]
+        lib.ref_get.argtypes = [C.c_char_p, _dp, C.c_long]
+        lib.ref_set.argtypes = [C.c_char_p, _dp, C.c_long]
+        lib.ref_set_interior_prims.argtypes = [_dp] * 5
+        lib.ref_rk3_step.argtypes = [C.c_double]
+        lib.ref_timestep.restype = C.c_double
+        lib.ref_total_energy.restype = C.c_double
+        lib.ref_params.argtypes = [_dp, C.POINTER(C.c_int)]
+        self.lib = lib
+        text = solver_in_text if solver_in_text is not None else format_solver_in(P, G)
+        with tempfile.NamedTemporaryFile("w", suffix=".in", delete=False) as f:
+            f.write(text)
+            path = f.name
+        try:
+            r = lib.ref_init_file(path.encode(), C.c_double(P.S_ref))
+        finally:
+            os.unlink(path)
+        if r != 0:
+            raise RuntimeError("reference parser failed")
+        self.nx, self.ny, self.nz = G.global_nx, G.global_ny, G.global_nz
+        self._get, self._set = lib.ref_get, lib.ref_set
+        self._set_interior = lib.ref_set_interior_prims
+
+    def params(self):
+        d = (C.c_double * 18)()
+        i = (C.c_int * 16)()
+        self.lib.ref_params(d, i)
+        return list(d), list(i)
+
+    def compute_rhs(self): self.lib.ref_compute_rhs()
+    def apply_boundary(self): self.lib.ref_apply_boundary()
+    def rk3_step(self, dt: float): self.lib.ref_rk3_step(C.c_double(dt))
+    def timestep(self) -> float: return self.lib.ref_timestep()
+    def total_energy(self) -> float: return self.lib.ref_total_energy()
+    def time_advance(self): self.lib.ref_time_advance()
