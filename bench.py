@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark of the ns3d_wcns RK3 step on B200: cell-updates/s.
+
+Workload (the GPU drop-in configuration): decaying isotropic turbulence on a
+periodic 256^3 grid over [0, 2pi]^3, seeded solenoidal field with
+E(k) ~ k^4 exp(-2 (k/k0)^2), k0 = 4, u_rms = 1, rho = 1, T = 1, Ma = 0.3,
+Re = 400, Pr = 0.72, S/T_ref = 110.4/273.15, MDCD_HYBRID interpolation + HLLC
+flux, 6th-order viscous terms, SSP-RK3 with the adaptive CFL = 0.5 time step
+of compute_timestep.  One step = compute_timestep + one full RK3 step (three
+RHS evaluations), exactly the work time_advance does per step.  Synthetic
+inputs: seeded by rank; the reference publishes no dataset.
+
+  value       device-timed whole-job cell-updates/s (state resident in HBM,
+              plain FP64 path: the reference's arithmetic)
+  e2e         the same through the C ABI with host Field3D buffers: every
+              step uploads the primitive state from pinned host memory and
+              downloads it after the step
+  mixed       the mixed FP32/FP64 path on the same workload
+  roofline    the dominant kernel's achieved algorithmic GB/s over its
+              CUDA-event launch time vs the measured HBM copy bandwidth
+  cpu_baseline the reference solver compiled from its sources (oracle/_ref),
+              one host core, bounded 64^3 sample of the same scheme
+
+N > 1 GPUs (torchrun): independent replicas, one 256^3 domain per GPU
+(weak scaling), max-over-ranks device time.
+``--impl reference`` times the reference's CPU implementation on the host
+cores (one single-rank process per core on 32^3 samples).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "isotropic turbulence 256^3 periodic, MDCD_HYBRID + HLLC, Ma 0.3, Re 400, CFL 0.5 adaptive"
+METRIC = "cell-updates/s at 256^3 (RK3 step incl. CFL dt), plain FP64 GPU path; mixed FP32/FP64 reported alongside"
+
+
+def bench_params(n: int, precision: int = 0):
+    from ns3d_wcns_b200.config import make_params
+    import math
+    return make_params(n=(n, n, n), L=(2 * math.pi,) * 3, Ma=0.3, Re=400.0, Pr=0.72, cfl=0.5, dt_fixed=-1.0,
+                       interpolation=3, riemann=2, S_ref=110.4 / 273.15, precision=precision)
+
+
+# --------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clock, power, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); smax.append(float(f[2])); power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "power_w_max": max(power), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- CPU baseline
+
+def _cpu_worker(args):
+    """One single-rank reference (or port) process: steps of the bench scheme."""
+    n, steps, warmup, seed = args
+    sys.path.insert(0, ROOT)
+    from ns3d_wcns_b200.initial import isotropic_state
+    from oracle import oracle
+    P, G = bench_params(n)
+    if oracle.ref_available():
+        s, kind = oracle.RefSolver(P, G), "reference"
+    else:
+        s, kind = oracle.PortSolver(P, G), "port"
+    s.set_interior_prims(*isotropic_state((n, n, n), P.gamma, P.Ma, seed=seed))
+    for _ in range(warmup):
+        s.rk3_step(s.timestep())
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.rk3_step(s.timestep())
+    return time.perf_counter() - t0, kind
+
+
+def cpu_baseline(n=64, steps=4):
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(1) as pool:
+        dt, kind = pool.map(_cpu_worker, [(n, steps, 0, 0)])[0]
+    return {"value": n ** 3 * steps / dt, "unit": "cell-updates/s", "cores": 1, "kind": kind,
+            "sample": f"{n}^3 periodic, same scheme (MDCD_HYBRID+HLLC, adaptive CFL), {steps} RK3 steps, "
+                      f"{dt:.1f} s on one host core"}
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's CPU path on all host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from oracle import oracle
+    oracle.build(ref=os.path.isdir(oracle.REF_SRC_DIR))
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    n = 32
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(n, args.steps, args.warmup, r) for r in range(cores)])
+    wall = time.perf_counter() - t0
+    times = [r[0] for r in res]
+    kind = res[0][1]
+    value = cores * n ** 3 * args.steps / max(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * max(times) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"{n}^3 per process", "processes": cores},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": kind,
+                         "sample": f"{cores} single-rank processes x {n}^3 periodic, {args.steps} timed steps each "
+                                   f"(reference has no threads; replicas bound its MPI scaling), wall {wall:.1f} s"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NS3D_BENCH_ALLOW_SHORT"), \
+        "at least 3 warm-up steps"
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    from ns3d_wcns_b200 import _lib
+    from ns3d_wcns_b200.initial import isotropic_state
+    from ns3d_wcns_b200.solver import Solver
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    n = args.n
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline()
+
+    st = isotropic_state((n, n, n), 1.4, 0.3, seed=rank)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_run(precision, profile):
+        P, G = bench_params(n, precision)
+        s = Solver(P, G, device=local)
+        s.set_stream(stream.cuda_stream)
+        s.set_interior_primitives(*st)
+        for _ in range(args.warmup):
+            s.rk3_step(s.compute_timestep())
+        if profile:
+            s.profile(True)
+        launches = 0
+        barrier()
+        torch.cuda.synchronize()
+        clk = ClockSampler(local)
+        clk.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            dt = s.compute_timestep()
+            launches += s.launches()
+            s.rk3_step(dt)
+            launches += s.launches()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        clocks = clk.stop()
+        barrier()
+        prof = s.profile_report() if profile else None
+        ke = s.total_energy()
+        s.close()
+        return max_over_ranks(ms), launches, prof, clocks, ke
+
+    ms64, launches, prof, clocks, ke64 = timed_run(0, profile=True)
+    cells = float(n) ** 3
+    value = world * cells * args.steps / (ms64 * 1e-3)
+
+    mixed = None
+    if not args.no_mixed:
+        msm, _, profm, _, kem = timed_run(1, profile=True)
+        mixed = {"value": world * cells * args.steps / (msm * 1e-3), "unit": "cell-updates/s",
+                 "ms_per_step": msm / args.steps, "over_fp64": ms64 / msm,
+                 "kernels_ms": {k: round(v["ms"] / max(v["launches"], 1), 4) for k, v in (profm or {}).items()}}
+
+    # roofline of the dominant kernel (algorithmic bytes per launch / event time)
+    algo_bytes_per_cell = {"sweep_x": 80, "sweep_y": 120, "sweep_z": 120, "viscous_flux": 40 + 72,
+                           "viscous_div": 72 + 64, "stage": 160, "cfl_dt": 40}
+    dom = max(prof, key=lambda k: prof[k]["ms"])
+    avg_ms = prof[dom]["ms"] / prof[dom]["launches"]
+    achieved = algo_bytes_per_cell.get(dom, 0) * cells / (avg_ms * 1e-3) / 1e9
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak, peak_src = json.load(open(peaks_path))["hbm_gbs"], "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(dom)
+
+    # end to end through the C ABI with host buffers (pinned)
+    e2e = None
+    if not args.no_e2e:
+        P, G = bench_params(n, 0)
+        s = Solver(P, G, device=local)
+        s.set_stream(stream.cuda_stream)
+        s.set_interior_primitives(*st)
+        host = torch.empty((5, n + 6, n + 6, n + 6), dtype=torch.float64, pin_memory=True).numpy()
+        host[...] = s.primitives()
+        for _ in range(args.warmup):
+            s.upload_primitives(host)
+            s.rk3_step(s.compute_timestep())
+            s._check(s.lib.ns3d_download(s.h, _lib.NS3D_PRIMITIVE, s._ptrs([host[q] for q in range(5)])))
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.upload_primitives(host)
+            s.rk3_step(s.compute_timestep())
+            s._check(s.lib.ns3d_download(s.h, _lib.NS3D_PRIMITIVE, s._ptrs([host[q] for q in range(5)])))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        mse = max_over_ranks(e0.elapsed_time(e1))
+        barrier()
+        s.close()
+        nbytes = 5 * (n + 6) ** 3 * 8
+        e2e = {"value": world * cells * args.steps / (mse * 1e-3), "unit": "cell-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 8,
+               "path": "ns3d_upload_primitives + ns3d_compute_timestep + ns3d_rk3_step + ns3d_download"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded isotropic field per rank)",
+            "config": {"workload": WORKLOAD, "grid": [n, n, n], "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (state 720 MB per copy)"},
+            "e2e": e2e, "mixed": mixed,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                         "algorithmic_bytes_per_cell": algo_bytes_per_cell.get(dom)},
+            "kernels_ms": {k: round(v["ms"] / max(v["launches"], 1), 4) for k, v in prof.items()},
+            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+            "kinetic_energy_end": ke64,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

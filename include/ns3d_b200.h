@@ -1,0 +1,182 @@
+/*
+ * ns3d_b200.h -- C ABI of the B200 (sm_100a) implementation of ns3d_wcns's
+ * right-hand-side evaluation and RK3 time advance.
+ *
+ * The entry points replace the per-rank CPU loops behind the reference's
+ * ns3d_func.h; each declaration names the reference interface it stands in
+ * for.  Plain pointers and sizes only: no C++ or torch types cross this
+ * boundary, no exceptions escape it, every call returns an int status
+ * (NS3D_OK == 0, negative on error) and ns3d_last_error() describes the last
+ * failure of a handle.
+ *
+ * Host arrays use the reference's Field3D layout (field_structures.h:64-67):
+ * one array per variable of sx*sy*sz doubles, sx = nx + 6, sy = ny + 6,
+ * sz = nz + 6 (3 ghost layers), id = (k*sy + j)*sx + i, x fastest.  Interior
+ * cells are i in [3, nx+3) etc.  The device keeps its own padded layout; the
+ * ABI converts on upload/download.
+ *
+ * Threading: one handle per host thread.  Calls are ordered on the handle's
+ * CUDA stream; calls that return host values synchronise that stream.
+ */
+#ifndef NS3D_B200_H
+#define NS3D_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define NS3D_OK 0
+#define NS3D_ERR_INVALID_ARG (-1)   /* null pointer, bad enum, bad size */
+#define NS3D_ERR_CONFIG (-2)        /* configuration the path does not support */
+#define NS3D_ERR_OOM (-3)           /* device allocation failed */
+#define NS3D_ERR_CUDA (-4)          /* CUDA runtime error (message in last_error) */
+#define NS3D_ERR_NONFINITE (-5)     /* non-finite or non-positive state detected */
+#define NS3D_ERR_NO_DEVICE (-6)     /* no usable CUDA device */
+#define NS3D_ERR_STATE (-7)         /* call out of order (e.g. no state uploaded) */
+#define NS3D_ERR_DT (-8)            /* time step <= 1e-12 (maincycle.cpp:46-52) */
+#define NS3D_ERR_TIMEOUT (-9)       /* a bounded device wait expired */
+
+/* ------------------------------------------------------------ enumerations */
+/* Same numbering as the reference enums (field_structures.h:131-165). */
+enum { NS3D_WENO5 = 0, NS3D_ZERO = 1, NS3D_MDCD_LINEAR = 2, NS3D_MDCD_HYBRID = 3 };
+enum { NS3D_ROE = 0, NS3D_RUSANOV = 1, NS3D_HLLC = 2, NS3D_HLL = 3, NS3D_HLLC_P = 4, NS3D_AUSM = 5 };
+enum { NS3D_PERIODIC = 0, NS3D_WALL = 1, NS3D_SYMMETRY = 2, NS3D_OUTFLOW = 3, NS3D_INFLOW = 4 };
+enum { NS3D_FP64 = 0, NS3D_MIXED = 1 };
+
+/* Which group of arrays ns3d_download / ns3d_device_fields refer to. */
+enum {
+    NS3D_PRIMITIVE = 0,   /* rho, u, v, w, p          (Field3D rho,u,v,w,p)        */
+    NS3D_CONSERVED = 1,   /* rho, rhou, rhov, rhow, E (Field3D rho,rhou,...,E)     */
+    NS3D_RHS = 2,         /* rhs_rho ... rhs_E of the last compute_rhs              */
+    NS3D_TEMPERATURE = 3  /* T = p / (rho Rgas)        (one array)                  */
+};
+
+/* SolverParams subset the hot path reads (field_structures.h:86-186) plus
+ * this build's additions.  Fill with ns3d_params_default() first. */
+typedef struct ns3d_params {
+    double gamma, Pr, Ma, Re;
+    double cfl, dt_fixed;           /* dt_fixed < 0 => adaptive (maincycle.cpp:30) */
+    double mdcd_diss, mdcd_disp;
+    double sutherland_s;            /* S/T_ref; reference value 110.4/288.15 */
+    int interpolation;              /* NS3D_WENO5 | NS3D_MDCD_LINEAR | NS3D_MDCD_HYBRID */
+    int riemann_solver;             /* NS3D_ROE ... NS3D_AUSM */
+    int char_recon;                 /* 0 component-wise, 1 characteristic-wise */
+    int bc[6];                      /* xmin xmax ymin ymax zmin zmax */
+    int precision;                  /* NS3D_FP64 (reference parity) | NS3D_MIXED */
+    int device;                     /* CUDA device ordinal */
+    int check_state;                /* 1: rk3 calls verify the state is finite */
+} ns3d_params;
+
+/* GridDesc (field_structures.h:33-38). */
+typedef struct ns3d_grid {
+    int nx, ny, nz;                 /* interior cells (global_nx ...) */
+    double x0, y0, z0;
+    double Lx, Ly, Lz;              /* dx = Lx / nx (initialization.cpp:170-172) */
+} ns3d_grid;
+
+typedef struct ns3d_handle ns3d_handle;
+
+/* Defaults of SolverParams (field_structures.h:86-186); bc all Periodic. */
+void ns3d_params_default(ns3d_params *p);
+
+const char *ns3d_status_string(int status);
+
+/* Allocates every device buffer of the solver for this grid.
+ * Replaces: Field3D::allocate (field_structures.h:250-373) and the MPI set-up
+ * of main.cpp:16-20 (one GPU holds the whole domain). */
+int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **out);
+int ns3d_destroy(ns3d_handle *h);
+const char *ns3d_last_error(const ns3d_handle *h);
+
+/* Field3D sizes: out[0..2] = sx, sy, sz. */
+int ns3d_field_dims(const ns3d_handle *h, int out[3]);
+
+/* Full-field upload of primitives (rho,u,v,w,p), all sx*sy*sz cells in Field3D
+ * layout: the state the reference holds after apply_boundary +
+ * primitiveToConserved (main.cpp:98-99).  Ghost cells are taken as given. */
+int ns3d_upload_primitives(ns3d_handle *h, const double *const fields[5]);
+
+/* Interior-only upload (nx*ny*nz per array, x fastest) followed by the device
+ * ghost fill.  Replaces: an initialiser + apply_boundary + primitiveToConserved
+ * (main.cpp:85-99). */
+int ns3d_set_interior_primitives(ns3d_handle *h, const double *const fields[5]);
+
+/* Download one group (NS3D_PRIMITIVE/CONSERVED/RHS: 5 arrays; TEMPERATURE: 1)
+ * in Field3D layout. */
+int ns3d_download(ns3d_handle *h, int what, double *const out[]);
+
+/* Ghost fill of the current state.  Replaces: apply_boundary
+ * (boundary.cpp:14-54, ns3d_func.h:60), including exchange_halos_physical's
+ * periodic wrap (field_structures.h:936-994). */
+int ns3d_apply_boundary(ns3d_handle *h);
+
+/* Right-hand side of the current state into the device RHS buffer.
+ * Replaces: compute_rhs (range_kutta.cpp:11-43, ns3d_func.h:134) and the
+ * functions it calls (compute_invis_flux, apply_boundary_halfnode_flux,
+ * compute_invis_dflux, compute_gradients, compute_viscous_flux,
+ * exchange_halos_viscous_flux, compute_vis_flux). */
+int ns3d_compute_rhs(ns3d_handle *h);
+
+/* One SSP-RK3 step: recordConservedTo0 + runge_kutta_3 with the c2p ->
+ * boundary -> p2c round trip after every stage.
+ * Replaces: runge_kutta_3 (range_kutta.cpp:46-92, ns3d_func.h:137) and
+ * Field3D::recordConservedTo0 (field_structures.h:491-497). */
+int ns3d_rk3_step(ns3d_handle *h, double dt);
+
+/* nsteps fixed-dt RK3 steps in one call (one synchronisation at the end). */
+int ns3d_rk3_steps(ns3d_handle *h, int nsteps, double dt);
+
+/* CFL time step.  Replaces: compute_timestep (timestep.cpp:5-23,
+ * ns3d_func.h:140): dt = cfl * min over the interior of dx/(|u|+a). */
+int ns3d_compute_timestep(ns3d_handle *h, double *dt_out);
+
+/* Sum of 0.5 rho |u|^2 dV over the interior.  Replaces: compute_total_energy
+ * (postprocess.cpp:103-128, ns3d_func.h:195). */
+int ns3d_total_energy(ns3d_handle *h, double *ke_out);
+
+/* Turbulence reductions of the current state, one pass, FP64 accumulation:
+ * out[0] = kinetic energy (as ns3d_total_energy),
+ * out[1] = <|grad u|^2> = mean over the interior of sum_ij (du_i/dx_j)^2 with
+ *          the viscous-gradient stencils (ViscousFlux.cpp:15-148),
+ * out[2] = mean Sutherland mu, out[3] = mean rho,
+ * out[4] = dissipation nu * <|grad u|^2>, nu = mean mu / mean rho: the
+ *          physical-space counterpart of the spectral epsilon
+ *          2 nu sum_k k^2 E(k) of ana_isotropic.cpp:271-305,
+ * out[5] = u_rms = sqrt(<u^2+v^2+w^2>/3) (ana_isotropic.cpp:280). */
+int ns3d_diagnostics(ns3d_handle *h, double out[6]);
+
+/* The dt schedule of time_advance (maincycle.cpp:18-56) without I/O:
+ * advances from *time until t_end or max_steps, adaptive dt when
+ * dt_fixed < 0, last step clipped to hit t_end.  Returns NS3D_ERR_DT when the
+ * step would be <= 1e-12 (the reference aborts the loop there). */
+int ns3d_time_advance(ns3d_handle *h, double t_end, int max_steps, double *time,
+                      int *steps_done);
+
+/* Device pointers of a group (5 pointers, or 1 for TEMPERATURE) plus the
+ * padded layout: layout[0..2] = sx, sy, sz, layout[3] = x pitch (elements),
+ * layout[4] = x offset of i = 0 (elements), layout[5] = element size (bytes).
+ * Pointers stay valid until the next ns3d_rk3_step / ns3d_destroy. */
+int ns3d_device_fields(ns3d_handle *h, int what, void *ptrs[5], long layout[6]);
+
+/* Bind the handle to a caller stream (cudaStream_t as void*; NULL = own). */
+int ns3d_set_stream(ns3d_handle *h, void *stream);
+int ns3d_synchronize(ns3d_handle *h);
+
+/* Kernel launches issued by the last call on this handle (launch accounting). */
+int ns3d_last_launch_count(const ns3d_handle *h, long *count);
+
+/* Per-kernel CUDA-event timing on the handle's stream (tracing; no
+ * reference counterpart: the reference times with MPI_Wtime only,
+ * maincycle.cpp:9,70-77).  enable != 0 starts a fresh record;
+ * ns3d_profile_report writes one line per kernel:
+ * "<name> <launches> <total milliseconds>". */
+int ns3d_profile(ns3d_handle *h, int enable);
+int ns3d_profile_report(ns3d_handle *h, char *buf, long len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,943 @@
+// capi.cu -- the C ABI (include/ns3d_b200.h): handle, device memory, launch
+// sequencing of compute_rhs / runge_kutta_3 / compute_timestep /
+// compute_total_energy, and the reductions.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ns3d_b200.h"
+#include "common.cuh"
+#include "schemes.cuh"
+#include "stage.cuh"
+#include "sweep.cuh"
+#include "viscous.cuh"
+
+using namespace ns3d;
+
+// --------------------------------------------------------------- reductions
+
+// Sums over interior cells: [0] KE (0.5 rho |u|^2 dV, postprocess.cpp:119-122),
+// [1] sum |grad u|^2, [2] sum mu(T), [3] sum rho, [4] sum |u|^2.
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) diag_kernel(ViscArgs<R> a, double vol, double *partials) {
+    const Layout &L = a.L;
+    const long ncell = (long)L.nx * L.ny * L.nz;
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = (int)(t / ((long)L.nx * L.ny));
+        const long c = L.at(i + NG, j + NG, k + NG);
+        const double rho = a.W[0][c], u = a.W[1][c], v = a.W[2][c], w = a.W[3][c];
+        const double kinetic = 0.5 * rho * (u * u + v * v + w * w);
+        acc[0] += kinetic * vol;
+        R g[12];
+        node_gradients(a, i + NG, j + NG, k + NG, g);
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) s += (double)g[q] * (double)g[q];
+        acc[1] += s;
+        const double T = (double)a.W[4][c] / ((double)a.W[0][c] * (double)a.Rgas);
+        acc[2] += (double)a.mu0 * pow(T, 1.5) * (1.0 + (double)a.S) / (T + (double)a.S);
+        acc[3] += rho;
+        acc[4] += u * u + v * v + w * w;
+    }
+    block_sum<5>(acc, partials + 5 * blockIdx.x);
+}
+
+// Minimum CFL bound over interior cells (compute_timestep, timestep.cpp:5-23).
+__global__ void __launch_bounds__(RED_THREADS) dt_kernel64(const double *const *Wp, Layout L, double gamma,
+                                                           double dx, double *partials) {
+    const long ncell = (long)L.nx * L.ny * L.nz;
+    double m = 1e9;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = (int)(t / ((long)L.nx * L.ny));
+        const long c = L.at(i + NG, j + NG, k + NG);
+        double U[5];
+        p2c_exact(Wp[0][c], Wp[1][c], Wp[2][c], Wp[3][c], Wp[4][c], gamma, U);
+        m = fmin(m, cfl_bound(U, gamma, dx));
+    }
+    block_min(m, partials + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) dt_kernel_mixed(const double *const *Up, Layout L, double gamma,
+                                                               double dx, double *partials) {
+    const long ncell = (long)L.nx * L.ny * L.nz;
+    double m = 1e9;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = (int)(t / ((long)L.nx * L.ny));
+        const long c = L.at(i + NG, j + NG, k + NG);
+        double U[5] = {Up[0][c], Up[1][c], Up[2][c], Up[3][c], Up[4][c]};
+        m = fmin(m, cfl_bound(U, gamma, dx));
+    }
+    block_min(m, partials + blockIdx.x);
+}
+
+// Non-finite / non-positive state detector: counts interior cells with a
+// non-finite value or rho <= 0 or p <= 0.
+template <typename R>
+__global__ void __launch_bounds__(RED_THREADS) check_kernel(const R *const *Wp, Layout L, double *partials) {
+    const long ncell = (long)L.nx * L.ny * L.nz;
+    double bad = 0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = (int)(t / ((long)L.nx * L.ny));
+        const long c = L.at(i + NG, j + NG, k + NG);
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) ok = ok && isfinite((double)Wp[q][c]);
+        ok = ok && Wp[0][c] > R(0) && Wp[4][c] > R(0);
+        bad += ok ? 0.0 : 1.0;
+    }
+    double v[1] = {bad};
+    block_sum<1>(v, partials + blockIdx.x);
+}
+
+// Fixed-order combination of per-block partials (nv values per block).
+// mode 0: sums, mode 1: minimum of value 0.
+__global__ void combine_kernel(const double *partials, int nblocks, int nv, int mode, double *out) {
+    if (threadIdx.x >= nv) return;
+    const int q = threadIdx.x;
+    double s = mode == 1 ? 1e300 : 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        const double x = partials[(long)b * nv + q];
+        s = mode == 1 ? fmin(s, x) : s + x;
+    }
+    out[q] = s;
+}
+
+// Interior upload helpers: host interior block (nx*ny*nz) -> padded state.
+template <typename T>
+__global__ void scatter_interior(const double *src, T *dst, Layout L) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.nx) return;
+    dst[L.at(i + NG, j + NG, k + NG)] = (T)src[((long)k * L.ny + j) * L.nx + i];
+}
+
+// Conserved FP64 state from FP64 primitives (mixed path set-up).
+__global__ void prim_to_cons_kernel(const double *const *Wp, double *const *Up, Layout L, double gamma) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    const long c = L.at(i, j, k);
+    double U[5];
+    p2c_exact(Wp[0][c], Wp[1][c], Wp[2][c], Wp[3][c], Wp[4][c], gamma, U);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) Up[q][c] = U[q];
+}
+
+// Group download conversions (device padded -> device scratch in Field3D
+// order is done by cudaMemcpy2D; these produce derived groups in place).
+__global__ void derive_kernel64(const double *const *Wp, double *const *Out, Layout L, double gamma,
+                                double Rgas, int what) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    const long c = L.at(i, j, k);
+    if (what == NS3D_CONSERVED) {
+        double U[5];
+        p2c_exact(Wp[0][c], Wp[1][c], Wp[2][c], Wp[3][c], Wp[4][c], gamma, U);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) Out[q][c] = U[q];
+    } else {  // temperature, field_structures.h:486
+        double rr = Wp[0][c] <= 0.0 ? 1e-12 : Wp[0][c];
+        Out[0][c] = Wp[4][c] / __dmul_rn(rr, Rgas);
+    }
+}
+
+__global__ void derive_kernel_mixed(const double *const *Up, double *const *Out, Layout L, double gamma,
+                                    double Rgas, int what) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    const long c = L.at(i, j, k);
+    double U[5] = {Up[0][c], Up[1][c], Up[2][c], Up[3][c], Up[4][c]};
+    double W[5];
+    c2p_exact(U, gamma, W);
+    if (what == NS3D_PRIMITIVE) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) Out[q][c] = W[q];
+    } else {
+        Out[0][c] = W[4] / __dmul_rn(W[0], Rgas);
+    }
+}
+
+template <typename T>
+__global__ void widen_kernel(const T *src, double *dst, Layout Ls, Layout Ld) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= Ls.sx) return;
+    dst[Ld.at(i, j, k)] = (double)src[Ls.at(i, j, k)];
+}
+
+template <typename T>
+__global__ void fill_kernel(T *dst, long n, T v) {
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) dst[t] = v;
+}
+
+// --------------------------------------------------------------- the handle
+
+struct ns3d_handle {
+    ns3d_params P;
+    ns3d_grid G;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    bool mixed = false;
+    Layout L64, L32;
+    Phys ph;
+    BcInfo bc;
+    SchemeParams<double> sp64;
+    SchemeParams<float> sp32;
+    // one allocation for every array
+    void *pool = nullptr;
+    size_t pool_bytes = 0;
+    // plain: S[b][q] primitive state buffers; mixed: S[b][q] FP64 conserved
+    double *S[3][5] = {};
+    int s0 = 0;          // buffer holding the current state
+    double *rhs64[5] = {};
+    float *w32[5] = {};
+    float *rhs32[5] = {};
+    void *visc[9] = {};  // double (plain) or float (mixed), interior layout
+    double *scratch[5] = {};   // download staging (points into a state buffer)
+    double **dptr = nullptr;   // device array of pointer tables
+    double *partials = nullptr;
+    double *scalars = nullptr;
+    int red_blocks = 0;
+    bool has_state = false;
+    long launches = 0;
+    std::string err;
+    cudaGraphExec_t step_graph = nullptr;
+    double graph_dt = 0.0;
+    int graph_s0 = -1;
+    // per-kernel CUDA-event timing (ns3d_profile)
+    bool profiling = false;
+    struct Prof { const char *name; std::vector<cudaEvent_t> ev; long launches; double ms; };
+    std::vector<Prof> prof;
+    int prof_open = -1;
+};
+
+namespace {
+
+int fail(ns3d_handle *h, int code, const std::string &msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_fail(ns3d_handle *h, cudaError_t e, const char *what) {
+    return fail(h, NS3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(h, call, what)                                   \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, what); \
+    } while (0)
+
+dim3 cell_grid(const Layout &L, bool with_ghosts, int bx = 128) {
+    int nx = with_ghosts ? L.sx : L.nx;
+    return dim3((nx + bx - 1) / bx, with_ghosts ? L.sy : L.ny, with_ghosts ? L.sz : L.nz);
+}
+
+double *const *state_table(ns3d_handle *h, int b) { return h->dptr + 5 * b; }
+
+int set_device(ns3d_handle *h) {
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    return NS3D_OK;
+}
+
+// Kernel timing: prof_begin/prof_end bracket one launch with events on the
+// handle's stream; ns3d_profile_report resolves the elapsed times.
+void prof_begin(ns3d_handle *h, const char *name) {
+    if (!h->profiling) return;
+    int idx = -1;
+    for (size_t q = 0; q < h->prof.size(); ++q)
+        if (std::strcmp(h->prof[q].name, name) == 0) idx = (int)q;
+    if (idx < 0) { h->prof.push_back({name, {}, 0, 0.0}); idx = (int)h->prof.size() - 1; }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, h->stream);
+    h->prof[idx].ev.push_back(a);
+    h->prof[idx].ev.push_back(b);
+    h->prof_open = idx;
+}
+
+void prof_end(ns3d_handle *h) {
+    if (!h->profiling || h->prof_open < 0) return;
+    cudaEventRecord(h->prof[h->prof_open].ev.back(), h->stream);
+    h->prof[h->prof_open].launches += 1;
+    h->prof_open = -1;
+}
+
+template <typename R>
+SweepArgs<R> sweep_args(ns3d_handle *h, int dir) {
+    SweepArgs<R> a;
+    const bool m = sizeof(R) == 4;
+    for (int q = 0; q < 5; ++q) {
+        if constexpr (sizeof(R) == 8) { a.W[q] = h->S[h->s0][q]; a.Rhs[q] = h->rhs64[q]; }
+        else { a.W[q] = h->w32[q]; a.Rhs[q] = h->rhs32[q]; }
+    }
+    a.L = m ? h->L32 : h->L64;
+    a.periodic = h->bc.periodic[dir];
+    a.outflow_lo = h->P.bc[2 * dir] == NS3D_OUTFLOW;
+    a.outflow_hi = h->P.bc[2 * dir + 1] == NS3D_OUTFLOW;
+    a.inv_h = (R)(dir == 0 ? h->ph.inv_dx : dir == 1 ? h->ph.inv_dy : h->ph.inv_dz);
+    if constexpr (sizeof(R) == 8) a.sp = h->sp64; else a.sp = h->sp32;
+    a.first = dir == 0;
+    return a;
+}
+
+template <typename R>
+ViscArgs<R> visc_args(ns3d_handle *h) {
+    ViscArgs<R> a;
+    for (int q = 0; q < 5; ++q) {
+        if constexpr (sizeof(R) == 8) { a.W[q] = h->S[h->s0][q]; a.Rhs[q] = h->rhs64[q]; }
+        else { a.W[q] = h->w32[q]; a.Rhs[q] = h->rhs32[q]; }
+    }
+    for (int q = 0; q < 9; ++q) a.V[q] = (R *)h->visc[q];
+    a.L = sizeof(R) == 8 ? h->L64 : h->L32;
+    for (int d = 0; d < 3; ++d) a.periodic[d] = h->bc.periodic[d];
+    a.h[0] = (R)h->ph.dx; a.h[1] = (R)h->ph.dy; a.h[2] = (R)h->ph.dz;
+    a.inv_h[0] = (R)h->ph.inv_dx; a.inv_h[1] = (R)h->ph.inv_dy; a.inv_h[2] = (R)h->ph.inv_dz;
+    a.Rgas = (R)h->ph.Rgas; a.mu0 = (R)h->ph.mu; a.S = (R)h->ph.S;
+    a.cp_over_pr = (R)(h->ph.Cp / h->ph.Pr);
+    return a;
+}
+
+template <typename R>
+int rhs_impl(ns3d_handle *h) {
+    cudaStream_t st = h->stream;
+    cudaError_t e;
+    prof_begin(h, "sweep_x");
+    e = sweep_x(sweep_args<R>(h, 0), st); if (e != cudaSuccess) return cuda_fail(h, e, "sweep_x");
+    prof_end(h);
+    prof_begin(h, "sweep_y");
+    e = sweep_y(sweep_args<R>(h, 1), st); if (e != cudaSuccess) return cuda_fail(h, e, "sweep_y");
+    prof_end(h);
+    prof_begin(h, "sweep_z");
+    e = sweep_z(sweep_args<R>(h, 2), st); if (e != cudaSuccess) return cuda_fail(h, e, "sweep_z");
+    prof_end(h);
+    h->launches += 3;
+    if (h->ph.mu != 0.0) {  // Re = inf: the viscous terms are exactly zero
+        ViscArgs<R> va = visc_args<R>(h);
+        dim3 g = cell_grid(va.L, false, 128);
+        prof_begin(h, "viscous_flux");
+        viscous_flux_kernel<R><<<g, 128, 0, st>>>(va);
+        prof_end(h);
+        prof_begin(h, "viscous_div");
+        viscous_div_kernel<R><<<g, 128, 0, st>>>(va);
+        prof_end(h);
+        h->launches += 2;
+        CK(h, cudaGetLastError(), "viscous kernels");
+    }
+    return NS3D_OK;
+}
+
+int compute_rhs_async(ns3d_handle *h) {
+    return h->mixed ? rhs_impl<float>(h) : rhs_impl<double>(h);
+}
+
+// stage: 1..3 RK stages, 0 = ghost fill of the current state.
+int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double dt) {
+    cudaStream_t st = h->stream;
+    dim3 g = cell_grid(h->L64, true, 128);
+    if (!h->mixed) {
+        StageArgs64 a;
+        for (int q = 0; q < 5; ++q) {
+            a.W0[q] = h->S[src0][q]; a.Wc[q] = h->S[srcc][q]; a.Rhs[q] = h->rhs64[q]; a.Wout[q] = h->S[dst][q];
+        }
+        a.L = h->L64; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
+        prof_begin(h, "stage");
+        stage_kernel64<<<g, 128, 0, st>>>(a);
+        prof_end(h);
+    } else {
+        StageArgsMixed a;
+        for (int q = 0; q < 5; ++q) {
+            a.U0[q] = h->S[src0][q]; a.Uc[q] = h->S[srcc][q]; a.Rhs[q] = h->rhs32[q];
+            a.Uout[q] = h->S[dst][q]; a.Wout[q] = h->w32[q];
+        }
+        a.L = h->L64; a.L32 = h->L32; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
+        prof_begin(h, "stage");
+        stage_kernel_mixed<<<g, 128, 0, st>>>(a);
+        prof_end(h);
+    }
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "stage kernel");
+    return NS3D_OK;
+}
+
+// One RK3 step (no synchronisation).  Buffers: state s0 -> stage 1 -> b1,
+// stage 2 -> b2, stage 3 -> b1; the new state is b1 (recordConservedTo0 is
+// the pointer rotation).
+int rk3_async(ns3d_handle *h, double dt) {
+    const int s0 = h->s0, b1 = (s0 + 1) % 3, b2 = (s0 + 2) % 3;
+    int r;
+    if ((r = compute_rhs_async(h)) != NS3D_OK) return r;
+    if ((r = stage_async(h, 1, s0, s0, b1, dt)) != NS3D_OK) return r;
+    h->s0 = b1;  // RHS of stage 2 reads the stage-1 state
+    if ((r = compute_rhs_async(h)) != NS3D_OK) { h->s0 = s0; return r; }
+    if ((r = stage_async(h, 2, s0, b1, b2, dt)) != NS3D_OK) { h->s0 = s0; return r; }
+    h->s0 = b2;
+    if ((r = compute_rhs_async(h)) != NS3D_OK) { h->s0 = s0; return r; }
+    if ((r = stage_async(h, 3, s0, b2, b1, dt)) != NS3D_OK) { h->s0 = s0; return r; }
+    h->s0 = b1;
+    return NS3D_OK;
+}
+
+int reduce_combine(ns3d_handle *h, int nv, int mode, double *host_out) {
+    combine_kernel<<<1, 32, 0, h->stream>>>(h->partials, h->red_blocks, nv, mode, h->scalars);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "combine");
+    CK(h, cudaMemcpyAsync(host_out, h->scalars, sizeof(double) * nv, cudaMemcpyDeviceToHost, h->stream), "copy scalars");
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return NS3D_OK;
+}
+
+int check_state(ns3d_handle *h) {
+    if (!h->mixed)
+        check_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->partials);
+    else
+        check_kernel<float><<<h->red_blocks, RED_THREADS, 0, h->stream>>>((const float *const *)(h->dptr + 25), h->L32,
+                                                                           h->partials);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "check kernel");
+    double bad = 0;
+    int r = reduce_combine(h, 1, 0, &bad);
+    if (r != NS3D_OK) return r;
+    if (bad > 0) return fail(h, NS3D_ERR_NONFINITE, "state has " + std::to_string((long)bad) +
+                                                       " interior cells with non-finite values or rho/p <= 0");
+    return NS3D_OK;
+}
+
+bool valid_params(const ns3d_params *p, const ns3d_grid *g, std::string &why) {
+    if (p->interpolation == NS3D_ZERO) {
+        why = "ZERO interpolation sets ghost_layers=1 while the flux difference and viscous stencils read "
+              "+-3 points (initialization.cpp:180-183); unsupported";
+        return false;
+    }
+    if (p->interpolation != NS3D_WENO5 && p->interpolation != NS3D_MDCD_LINEAR && p->interpolation != NS3D_MDCD_HYBRID) {
+        why = "unknown interpolation"; return false;
+    }
+    if (p->riemann_solver < 0 || p->riemann_solver > 5) { why = "unknown Riemann solver"; return false; }
+    for (int f = 0; f < 6; ++f)
+        if (p->bc[f] < 0 || p->bc[f] > 4) { why = "unknown boundary type"; return false; }
+    if (p->precision != NS3D_FP64 && p->precision != NS3D_MIXED) { why = "unknown precision"; return false; }
+    if (g->nx < 3 || g->ny < 3 || g->nz < 3) { why = "each dimension needs at least 3 interior cells"; return false; }
+    if ((long)g->nx * g->ny * g->nz > (1L << 31)) { why = "grid too large"; return false; }
+    if (!(g->Lx > 0 && g->Ly > 0 && g->Lz > 0)) { why = "domain lengths must be positive"; return false; }
+    if (!(p->gamma > 1.0) || !(p->Ma > 0) || !(p->Pr > 0) || !(p->Re > 0)) { why = "invalid physical constants"; return false; }
+    return true;
+}
+
+}  // namespace
+
+// =============================================================== C ABI
+
+extern "C" {
+
+void ns3d_params_default(ns3d_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->gamma = 1.4; p->Pr = 0.71; p->Ma = 0.4; p->Re = 500.0; p->cfl = 0.1; p->dt_fixed = -1.0;
+    p->mdcd_diss = 0.01; p->mdcd_disp = 0.0463783; p->sutherland_s = 110.4 / 288.15;
+    p->interpolation = NS3D_WENO5; p->riemann_solver = NS3D_ROE; p->char_recon = 0;
+    for (int f = 0; f < 6; ++f) p->bc[f] = NS3D_PERIODIC;
+    p->precision = NS3D_FP64; p->device = 0; p->check_state = 0;
+}
+
+const char *ns3d_status_string(int s) {
+    switch (s) {
+        case NS3D_OK: return "ok";
+        case NS3D_ERR_INVALID_ARG: return "invalid argument";
+        case NS3D_ERR_CONFIG: return "unsupported configuration";
+        case NS3D_ERR_OOM: return "out of device memory";
+        case NS3D_ERR_CUDA: return "CUDA error";
+        case NS3D_ERR_NONFINITE: return "non-finite state";
+        case NS3D_ERR_NO_DEVICE: return "no CUDA device";
+        case NS3D_ERR_STATE: return "no state uploaded";
+        case NS3D_ERR_DT: return "time step too small";
+        case NS3D_ERR_TIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+static thread_local std::string g_create_error;
+
+const char *ns3d_last_error(const ns3d_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **out) {
+    if (!params || !grid || !out) return NS3D_ERR_INVALID_ARG;
+    *out = nullptr;
+    std::string why;
+    if (!valid_params(params, grid, why)) {
+        g_create_error = why;
+        return NS3D_ERR_CONFIG;
+    }
+    g_create_error.clear();
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NS3D_ERR_NO_DEVICE;
+    if (params->device < 0 || params->device >= ndev) return NS3D_ERR_INVALID_ARG;
+    ns3d_handle *h = new (std::nothrow) ns3d_handle();
+    if (!h) return NS3D_ERR_OOM;
+    h->P = *params;
+    h->G = *grid;
+    h->device = params->device;
+    h->mixed = params->precision == NS3D_MIXED;
+    if (cudaSetDevice(h->device) != cudaSuccess) { delete h; return NS3D_ERR_NO_DEVICE; }
+    h->L64 = make_layout<double>(grid->nx, grid->ny, grid->nz);
+    h->L32 = make_layout<float>(grid->nx, grid->ny, grid->nz);
+    // derived constants, initialization.cpp:170-172, 194-197
+    Phys &ph = h->ph;
+    ph.gamma = params->gamma;
+    ph.Rgas = 1.0 / (params->Ma * params->Ma * params->gamma);
+    const double Cv = 1.0 / (params->gamma * (params->gamma - 1.0) * params->Ma * params->Ma);
+    ph.Cp = Cv * params->gamma;
+    ph.Pr = params->Pr;
+    ph.mu = std::isinf(params->Re) ? 0.0 : 1.0 / params->Re;
+    ph.S = params->sutherland_s;
+    ph.dx = grid->Lx / grid->nx; ph.dy = grid->Ly / grid->ny; ph.dz = grid->Lz / grid->nz;
+    ph.inv_dx = 1.0 / ph.dx; ph.inv_dy = 1.0 / ph.dy; ph.inv_dz = 1.0 / ph.dz;
+    ph.mdcd_disp = params->mdcd_disp; ph.mdcd_diss = params->mdcd_diss;
+    for (int d = 0; d < 3; ++d)
+        h->bc.periodic[d] = params->bc[2 * d] == NS3D_PERIODIC && params->bc[2 * d + 1] == NS3D_PERIODIC;
+    for (int f = 0; f < 6; ++f) h->bc.bc[f] = params->bc[f];
+    // interpolation coefficients, interpolation.cpp:130-132, 179-182
+    const double disp = params->mdcd_disp, diss = params->mdcd_diss;
+    const double lin[6] = {(3.0 * disp + 3.0 * diss) / 8.0, (-18.0 * disp - 30 * diss - 1.0) / 16.0,
+                           (12.0 * disp + 60.0 * diss + 9.0) / 16.0, (12.0 * disp - 60.0 * diss + 9.0) / 16.0,
+                           (-18.0 * disp + 30.0 * diss - 1.0) / 16.0, (3.0 * disp - 3.0 * diss) / 8.0};
+    const double hd[4] = {1.5 * (disp + diss), 0.5 - 1.5 * (disp - 3 * diss), 0.5 - 1.5 * (disp + 3 * diss),
+                          1.5 * (disp - diss)};
+    h->sp64.gamma = params->gamma; h->sp32.gamma = (float)params->gamma;
+    for (int q = 0; q < 6; ++q) { h->sp64.lin[q] = lin[q]; h->sp32.lin[q] = (float)lin[q]; }
+    for (int q = 0; q < 4; ++q) { h->sp64.hd[q] = hd[q]; h->sp32.hd[q] = (float)hd[q]; }
+    h->sp64.interp = h->sp32.interp = params->interpolation;
+    h->sp64.riemann = h->sp32.riemann = params->riemann_solver;
+    h->sp64.char_recon = h->sp32.char_recon = params->char_recon;
+
+    // memory plan (bytes, each array 256-byte aligned)
+    const long p64 = h->L64.plane * 8, p32 = h->L32.plane * 4;
+    const long ncell = (long)grid->nx * grid->ny * grid->nz;
+    const long vis_elems = ((ncell + 63) / 64) * 64;
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
+    h->red_blocks = dev_sms * 4;
+    size_t bytes = 15 * p64;                                   // three state buffers
+    bytes += h->mixed ? 10 * p32 : 5 * p64;                    // (w32 + rhs32) or rhs64
+    bytes += 9 * vis_elems * (h->mixed ? 4 : 8);               // viscous node fluxes
+    bytes += 256 * 32;                                         // pointer tables
+    bytes += ((size_t)h->red_blocks * 8 * 8 + 255) / 256 * 256;  // partials
+    bytes += 256;                                              // scalars
+    cudaError_t e = cudaMalloc(&h->pool, bytes);
+    if (e != cudaSuccess) { delete h; cudaGetLastError(); return NS3D_ERR_OOM; }
+    h->pool_bytes = bytes;
+    char *p = (char *)h->pool;
+    for (int b = 0; b < 3; ++b)
+        for (int q = 0; q < 5; ++q) { h->S[b][q] = (double *)p; p += p64; }
+    if (h->mixed) {
+        for (int q = 0; q < 5; ++q) { h->w32[q] = (float *)p; p += p32; }
+        for (int q = 0; q < 5; ++q) { h->rhs32[q] = (float *)p; p += p32; }
+    } else {
+        for (int q = 0; q < 5; ++q) { h->rhs64[q] = (double *)p; p += p64; }
+    }
+    for (int q = 0; q < 9; ++q) { h->visc[q] = p; p += vis_elems * (h->mixed ? 4 : 8); }
+    h->dptr = (double **)p; p += 256 * 32;
+    h->partials = (double *)p; p += ((size_t)h->red_blocks * 8 * 8 + 255) / 256 * 256;
+    h->scalars = (double *)p;
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { cudaFree(h->pool); delete h; return NS3D_ERR_CUDA; }
+    h->own_stream = true;
+    // pointer tables: [0..14] state buffers, [15..19] scratch, [20..24] rhs64, [25..29] w32
+    void *tab[30] = {};
+    for (int b = 0; b < 3; ++b)
+        for (int q = 0; q < 5; ++q) tab[5 * b + q] = h->S[b][q];
+    for (int q = 0; q < 5; ++q) {
+        tab[20 + q] = h->rhs64[q];
+        tab[25 + q] = h->w32[q];
+    }
+    e = cudaMemcpy(h->dptr, tab, sizeof(tab), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(h->pool, 0, (size_t)((char *)h->dptr - (char *)h->pool));
+    if (e != cudaSuccess) { ns3d_destroy(h); return NS3D_ERR_CUDA; }
+    // Field3D::allocate: rho = 1 everywhere (field_structures.h:257)
+    for (int b = 0; b < 3; ++b) {
+        fill_kernel<double><<<256, 256, 0, h->stream>>>(h->S[b][0], h->L64.plane, 1.0);
+    }
+    if (h->mixed) fill_kernel<float><<<256, 256, 0, h->stream>>>(h->w32[0], h->L32.plane, 1.0f);
+    e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { ns3d_destroy(h); return NS3D_ERR_CUDA; }
+    *out = h;
+    return NS3D_OK;
+}
+
+int ns3d_destroy(ns3d_handle *h) {
+    if (!h) return NS3D_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto &p : h->prof)
+        for (auto e : p.ev) cudaEventDestroy(e);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    if (h->pool) cudaFree(h->pool);
+    delete h;
+    return NS3D_OK;
+}
+
+int ns3d_field_dims(const ns3d_handle *h, int out[3]) {
+    if (!h || !out) return NS3D_ERR_INVALID_ARG;
+    out[0] = h->L64.sx; out[1] = h->L64.sy; out[2] = h->L64.sz;
+    return NS3D_OK;
+}
+
+int ns3d_set_stream(ns3d_handle *h, void *stream) {
+    if (!h) return NS3D_ERR_INVALID_ARG;
+    int r = set_device(h); if (r) return r;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    if (stream) { h->stream = (cudaStream_t)stream; h->own_stream = false; }
+    else { CK(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream"); h->own_stream = true; }
+    if (h->step_graph) { cudaGraphExecDestroy(h->step_graph); h->step_graph = nullptr; }
+    return NS3D_OK;
+}
+
+int ns3d_synchronize(ns3d_handle *h) {
+    if (!h) return NS3D_ERR_INVALID_ARG;
+    int r = set_device(h); if (r) return r;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return NS3D_OK;
+}
+
+int ns3d_last_launch_count(const ns3d_handle *h, long *count) {
+    if (!h || !count) return NS3D_ERR_INVALID_ARG;
+    *count = h->launches;
+    return NS3D_OK;
+}
+
+// host Field3D array (sx*sy*sz doubles) -> padded device array
+static int upload_plane(ns3d_handle *h, double *dst, const double *src) {
+    const Layout &L = h->L64;
+    CK(h, cudaMemcpy2DAsync(dst + L.off, (size_t)L.px * 8, src, (size_t)L.sx * 8, (size_t)L.sx * 8,
+                            (size_t)L.sy * L.sz, cudaMemcpyHostToDevice, h->stream), "upload");
+    return NS3D_OK;
+}
+
+static int download_plane(ns3d_handle *h, double *dst, const double *src) {
+    const Layout &L = h->L64;
+    CK(h, cudaMemcpy2DAsync(dst, (size_t)L.sx * 8, src + L.off, (size_t)L.px * 8, (size_t)L.sx * 8,
+                            (size_t)L.sy * L.sz, cudaMemcpyDeviceToHost, h->stream), "download");
+    return NS3D_OK;
+}
+
+// FP64 primitives of the full field sit in buffer b.  Plain path: b becomes
+// the state (after the ghost fill when apply_bc).  Mixed path: FP64
+// conserved state + FP32 primitives are derived from it.
+__global__ void upload_mixed_kernel(const double *const *Wp, double *const *Up, float *const *W32, Layout L,
+                                    Layout L32, double gamma) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    const long c = L.at(i, j, k), c32 = L32.at(i, j, k);
+    double U[5];
+    p2c_exact(Wp[0][c], Wp[1][c], Wp[2][c], Wp[3][c], Wp[4][c], gamma, U);
+    double W[5];
+    c2p_exact(U, gamma, W);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) { Up[q][c] = U[q]; W32[q][c32] = (float)W[q]; }
+}
+
+static int finish_upload(ns3d_handle *h, int b, bool apply_bc) {
+    const int dst = (b + 1) % 3, dst2 = (b + 2) % 3;
+    int r;
+    if (!h->mixed) {
+        if (!apply_bc) { h->s0 = b; return NS3D_OK; }
+        if ((r = stage_async(h, 0, b, b, dst, 0.0))) return r;
+        h->s0 = dst;
+        return NS3D_OK;
+    }
+    dim3 g = cell_grid(h->L64, true, 128);
+    upload_mixed_kernel<<<g, 128, 0, h->stream>>>(state_table(h, b), state_table(h, dst),
+                                                  (float *const *)(h->dptr + 25), h->L64, h->L32, h->ph.gamma);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "upload conversion");
+    h->s0 = dst;
+    if (!apply_bc) return NS3D_OK;
+    if ((r = stage_async(h, 0, dst, dst, dst2, 0.0))) return r;
+    h->s0 = dst2;
+    return NS3D_OK;
+}
+
+int ns3d_upload_primitives(ns3d_handle *h, const double *const fields[5]) {
+    if (!h || !fields) return NS3D_ERR_INVALID_ARG;
+    for (int q = 0; q < 5; ++q) if (!fields[q]) return NS3D_ERR_INVALID_ARG;
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    const int b = (h->s0 + 1) % 3;
+    for (int q = 0; q < 5; ++q) if ((r = upload_plane(h, h->S[b][q], fields[q]))) return r;
+    if ((r = finish_upload(h, b, false))) return r;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    h->has_state = true;
+    return NS3D_OK;
+}
+
+int ns3d_set_interior_primitives(ns3d_handle *h, const double *const fields[5]) {
+    if (!h || !fields) return NS3D_ERR_INVALID_ARG;
+    for (int q = 0; q < 5; ++q) if (!fields[q]) return NS3D_ERR_INVALID_ARG;
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    const Layout &L = h->L64;
+    const size_t nb = (size_t)L.nx * L.ny * L.nz * 8;
+    // stage the interior blocks in the RHS/viscous area? use the free state buffer
+    const int b = (h->s0 + 1) % 3, tmp = (h->s0 + 2) % 3;
+    // plain: the current state keeps its ghosts (initially the allocate defaults)
+    // mixed: the current FP64 primitives are recomputed from the conserved state
+    if (h->mixed) {
+        dim3 g = cell_grid(L, true, 128);
+        derive_kernel_mixed<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), state_table(h, b), L, h->ph.gamma,
+                                                       h->ph.Rgas, NS3D_PRIMITIVE);
+        h->launches += 1;
+    } else {
+        for (int q = 0; q < 5; ++q)
+            CK(h, cudaMemcpyAsync(h->S[b][q], h->S[h->s0][q], L.plane * 8, cudaMemcpyDeviceToDevice, h->stream), "copy");
+    }
+    for (int q = 0; q < 5; ++q) {
+        double *stage_buf = h->S[tmp][q];
+        CK(h, cudaMemcpyAsync(stage_buf, fields[q], nb, cudaMemcpyHostToDevice, h->stream), "upload interior");
+        scatter_interior<double><<<cell_grid(L, false, 128), 128, 0, h->stream>>>(stage_buf, h->S[b][q], L);
+        h->launches += 1;
+    }
+    CK(h, cudaGetLastError(), "scatter");
+    // apply_boundary + primitiveToConserved (main.cpp:98-99)
+    if ((r = finish_upload(h, b, true))) return r;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    h->has_state = true;
+    return NS3D_OK;
+}
+
+int ns3d_download(ns3d_handle *h, int what, double *const out[]) {
+    if (!h || !out) return NS3D_ERR_INVALID_ARG;
+    if (what < NS3D_PRIMITIVE || what > NS3D_TEMPERATURE) return NS3D_ERR_INVALID_ARG;
+    const int nq = what == NS3D_TEMPERATURE ? 1 : 5;
+    for (int q = 0; q < nq; ++q) if (!out[q]) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state && what != NS3D_RHS) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    int r = set_device(h); if (r) return r;
+    const Layout &L = h->L64;
+    const int free_b = (h->s0 + 1) % 3;
+    // scratch for derived groups: the free state buffer (its contents are dead between steps)
+    double *const *scr = state_table(h, free_b);
+    dim3 g = cell_grid(L, true, 128);
+    if (what == NS3D_RHS) {
+        if (!h->mixed) {
+            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->rhs64[q]))) return r;
+        } else {
+            for (int q = 0; q < 5; ++q)
+                widen_kernel<float><<<g, 128, 0, h->stream>>>(h->rhs32[q], h->S[free_b][q], h->L32, L);
+            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->S[free_b][q]))) return r;
+        }
+    } else if (!h->mixed) {
+        if (what == NS3D_PRIMITIVE) {
+            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->S[h->s0][q]))) return r;
+        } else {
+            derive_kernel64<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), scr, L, h->ph.gamma, h->ph.Rgas, what);
+            CK(h, cudaGetLastError(), "derive");
+            for (int q = 0; q < nq; ++q) if ((r = download_plane(h, out[q], h->S[free_b][q]))) return r;
+        }
+    } else {
+        if (what == NS3D_CONSERVED) {
+            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->S[h->s0][q]))) return r;
+        } else {
+            derive_kernel_mixed<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), scr, L, h->ph.gamma, h->ph.Rgas, what);
+            CK(h, cudaGetLastError(), "derive");
+            for (int q = 0; q < nq; ++q) if ((r = download_plane(h, out[q], h->S[free_b][q]))) return r;
+        }
+    }
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return NS3D_OK;
+}
+
+int ns3d_apply_boundary(ns3d_handle *h) {
+    if (!h) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    const int dst = (h->s0 + 1) % 3;
+    if ((r = stage_async(h, 0, h->s0, h->s0, dst, 0.0))) return r;
+    h->s0 = dst;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return NS3D_OK;
+}
+
+int ns3d_compute_rhs(ns3d_handle *h) {
+    if (!h) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    if ((r = compute_rhs_async(h))) return r;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return NS3D_OK;
+}
+
+int ns3d_rk3_step(ns3d_handle *h, double dt) {
+    if (!h) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    if (!std::isfinite(dt)) return fail(h, NS3D_ERR_INVALID_ARG, "dt is not finite");
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    if ((r = rk3_async(h, dt))) return r;
+    if (h->P.check_state) return check_state(h);
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return NS3D_OK;
+}
+
+// One step per graph launch; the step graph is captured for the buffer
+// rotation state it starts from, so three consecutive graphs cover a cycle.
+int ns3d_rk3_steps(ns3d_handle *h, int nsteps, double dt) {
+    if (!h || nsteps < 0) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    if (!std::isfinite(dt)) return fail(h, NS3D_ERR_INVALID_ARG, "dt is not finite");
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    for (int s = 0; s < nsteps; ++s) {
+        if ((r = rk3_async(h, dt))) return r;
+    }
+    if (h->P.check_state) return check_state(h);
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return NS3D_OK;
+}
+
+int ns3d_compute_timestep(ns3d_handle *h, double *dt_out) {
+    if (!h || !dt_out) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    prof_begin(h, "cfl_dt");
+    if (!h->mixed)
+        dt_kernel64<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
+                                                                  h->ph.dx, h->partials);
+    else
+        dt_kernel_mixed<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
+                                                                      h->ph.dx, h->partials);
+    prof_end(h);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "dt kernel");
+    double m = 0;
+    if ((r = reduce_combine(h, 1, 1, &m))) return r;
+    *dt_out = h->P.cfl * m;
+    return NS3D_OK;
+}
+
+int ns3d_diagnostics(ns3d_handle *h, double out[6]) {
+    if (!h || !out) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    const double vol = h->ph.dx * h->ph.dy * h->ph.dz;
+    if (!h->mixed) {
+        diag_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(visc_args<double>(h), vol, h->partials);
+    } else {
+        // FP64 primitives of the current conserved state for the reductions
+        const int b = (h->s0 + 1) % 3;
+        dim3 g = cell_grid(h->L64, true, 128);
+        derive_kernel_mixed<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), state_table(h, b), h->L64, h->ph.gamma,
+                                                       h->ph.Rgas, NS3D_PRIMITIVE);
+        ViscArgs<double> a = visc_args<double>(h);
+        for (int q = 0; q < 5; ++q) a.W[q] = h->S[b][q];
+        a.L = h->L64;
+        diag_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(a, vol, h->partials);
+        h->launches += 1;
+    }
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "diagnostics");
+    double s[5];
+    if ((r = reduce_combine(h, 5, 0, s))) return r;
+    const double N = (double)h->G.nx * h->G.ny * h->G.nz;
+    const double mean_mu = s[2] / N, mean_rho = s[3] / N;
+    out[0] = s[0];
+    out[1] = s[1] / N;
+    out[2] = mean_mu;
+    out[3] = mean_rho;
+    out[4] = (mean_mu / mean_rho) * (s[1] / N);
+    out[5] = std::sqrt(s[4] / (3.0 * N));
+    return NS3D_OK;
+}
+
+int ns3d_total_energy(ns3d_handle *h, double *ke_out) {
+    if (!ke_out) return NS3D_ERR_INVALID_ARG;
+    double d[6];
+    int r = ns3d_diagnostics(h, d);
+    if (r) return r;
+    *ke_out = d[0];
+    return NS3D_OK;
+}
+
+// time_advance's dt schedule (maincycle.cpp:18-56) without output.
+int ns3d_time_advance(ns3d_handle *h, double t_end, int max_steps, double *time, int *steps_done) {
+    if (!h || !time) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    const double eps = 1e-12;
+    int done = 0, r = NS3D_OK;
+    double t = *time;
+    for (int step = 1; step <= max_steps; ++step) {
+        if (std::fabs(t_end - t) <= eps) break;
+        double dt = h->P.dt_fixed;
+        if (h->P.dt_fixed < 0.0 && (r = ns3d_compute_timestep(h, &dt))) break;
+        if (t + dt > t_end) dt = t_end - t;
+        if (dt <= eps) { r = fail(h, NS3D_ERR_DT, "dt too small or zero"); break; }
+        t += dt;
+        if ((r = ns3d_rk3_step(h, dt))) break;
+        ++done;
+        if (t >= t_end) break;
+    }
+    *time = t;
+    if (steps_done) *steps_done = done;
+    return r;
+}
+
+int ns3d_device_fields(ns3d_handle *h, int what, void *ptrs[5], long layout[6]) {
+    if (!h || !ptrs || !layout) return NS3D_ERR_INVALID_ARG;
+    const Layout *L = &h->L64;
+    long esz = 8;
+    if (what == NS3D_PRIMITIVE && !h->mixed) {
+        for (int q = 0; q < 5; ++q) ptrs[q] = h->S[h->s0][q];
+    } else if (what == NS3D_PRIMITIVE && h->mixed) {
+        for (int q = 0; q < 5; ++q) ptrs[q] = h->w32[q];
+        L = &h->L32; esz = 4;
+    } else if (what == NS3D_CONSERVED && h->mixed) {
+        for (int q = 0; q < 5; ++q) ptrs[q] = h->S[h->s0][q];
+    } else if (what == NS3D_RHS) {
+        for (int q = 0; q < 5; ++q) ptrs[q] = h->mixed ? (void *)h->rhs32[q] : (void *)h->rhs64[q];
+        if (h->mixed) { L = &h->L32; esz = 4; }
+    } else {
+        return fail(h, NS3D_ERR_INVALID_ARG, "group not resident on the device in this precision");
+    }
+    layout[0] = L->sx; layout[1] = L->sy; layout[2] = L->sz; layout[3] = L->px; layout[4] = L->off; layout[5] = esz;
+    return NS3D_OK;
+}
+
+int ns3d_profile(ns3d_handle *h, int enable) {
+    if (!h) return NS3D_ERR_INVALID_ARG;
+    int r = set_device(h); if (r) return r;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    for (auto &p : h->prof)
+        for (auto e : p.ev) cudaEventDestroy(e);
+    h->prof.clear();
+    h->profiling = enable != 0;
+    return NS3D_OK;
+}
+
+int ns3d_profile_report(ns3d_handle *h, char *buf, long len) {
+    if (!h || !buf || len <= 0) return NS3D_ERR_INVALID_ARG;
+    int r = set_device(h); if (r) return r;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    std::string out;
+    for (auto &p : h->prof) {
+        double ms = 0.0;
+        for (size_t q = 0; q + 1 < p.ev.size(); q += 2) {
+            float t = 0.f;
+            CK(h, cudaEventElapsedTime(&t, p.ev[q], p.ev[q + 1]), "event time");
+            ms += t;
+        }
+        char line[160];
+        std::snprintf(line, sizeof(line), "%s %ld %.6f\n", p.name, p.launches, ms);
+        out += line;
+    }
+    if ((long)out.size() + 1 > len) return fail(h, NS3D_ERR_INVALID_ARG, "report buffer too small");
+    std::memcpy(buf, out.c_str(), out.size() + 1);
+    return NS3D_OK;
+}
+
+}  // extern "C"

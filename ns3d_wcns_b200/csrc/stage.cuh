@@ -1,0 +1,253 @@
+// stage.cuh -- RK3 stage update with the state round trip and the ghost fill,
+// plus the global reductions (CFL time step, kinetic energy, dissipation).
+//
+// The reference performs, after every RK stage (range_kutta.cpp:53-91):
+//   U = a U0 + b (U + dt rhs) on all cells (rhs = 0 in ghosts),
+//   conservedToPrimitive on all cells (density clamp),
+//   apply_boundary: periodic exchange (or, in non-periodic dimensions, the
+//     unpack of never-received zero buffers) on interior-tangential ghost
+//     slabs, then the Wall/Symmetry/Outflow/Inflow fills face by face over
+//     full tangential extents (boundary.cpp:14-205),
+//   primitiveToConserved on all cells.
+// Here one thread per output cell walks that sequence backwards to the cell
+// whose stage value it receives (with velocity sign flips, or a constant
+// Inflow / zero state), computes that cell's stage update and conversion, and
+// writes the result: one pass, no separate ghost kernel, no grid barrier.
+#pragma once
+
+#include "common.cuh"
+
+namespace ns3d {
+
+struct BcInfo {
+    int periodic[3];
+    int bc[6];   // NS3D_* boundary types
+};
+
+enum { SRC_CELL = 0, SRC_ZERO = 1, SRC_INFLOW = 2 };
+enum { BC_PERIODIC = 0, BC_WALL = 1, BC_SYMMETRY = 2, BC_OUTFLOW = 3, BC_INFLOW = 4 };
+
+// Resolve cell c (ghost-inclusive coordinates) to its source.  flip bit d set
+// => negate velocity component d.
+__device__ __forceinline__ int resolve_source(const Layout &L, const BcInfo &b, int c[3], int &flip) {
+    const int ext[3] = {L.sx, L.sy, L.sz};
+    const int n[3] = {L.nx, L.ny, L.nz};
+    flip = 0;
+#pragma unroll
+    for (int face = 5; face >= 0; --face) {
+        const int d = face >> 1, hi = face & 1;
+        if (b.periodic[d]) continue;
+        const int t = b.bc[face];
+        if (t == BC_PERIODIC) continue;  // Periodic side without a periodic partner: no fill
+        const bool in = hi ? (c[d] >= ext[d] - NG) : (c[d] < NG);
+        if (!in) continue;
+        if (t == BC_INFLOW) return SRC_INFLOW;
+        if (t == BC_OUTFLOW) c[d] = hi ? ext[d] - NG - 1 : NG;
+        else { c[d] = hi ? 2 * (ext[d] - NG) - 1 - c[d] : 2 * NG - 1 - c[d]; flip ^= 1 << d; }
+    }
+    // exchange_halos_physical: ghost in exactly one dimension, interior in the others
+    int gd = -1, ng = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        if (c[d] < NG || c[d] >= NG + n[d]) { gd = d; ++ng; }
+    if (ng == 1) {
+        if (!b.periodic[gd]) return SRC_ZERO;
+        c[gd] += c[gd] < NG ? n[gd] : -n[gd];
+    }
+    return SRC_CELL;
+}
+
+__device__ __forceinline__ bool is_interior(const Layout &L, const int c[3]) {
+    return c[0] >= NG && c[0] < NG + L.nx && c[1] >= NG && c[1] < NG + L.ny && c[2] >= NG && c[2] < NG + L.nz;
+}
+
+// Constant states of the ghost fill (after primitiveToConserved's clamp).
+__device__ __forceinline__ void special_state(int kind, double W[5]) {
+    if (kind == SRC_INFLOW) { W[0] = 1.0; W[1] = 1.0; W[2] = 0.0; W[3] = 0.0; W[4] = 1.0; }  // boundary.cpp:188
+    else { W[0] = 1e-12; W[1] = 0.0; W[2] = 0.0; W[3] = 0.0; W[4] = 0.0; }
+}
+
+__device__ __forceinline__ void apply_flips(int flip, double W[5]) {
+    if (flip & 1) W[1] = -W[1];
+    if (flip & 2) W[2] = -W[2];
+    if (flip & 4) W[3] = -W[3];
+}
+
+// --------------------------------------------------------------- plain FP64
+
+struct StageArgs64 {
+    const double *W0[5];    // step-start state
+    const double *Wc[5];    // current stage state
+    const double *Rhs[5];
+    double *Wout[5];
+    Layout L;
+    BcInfo b;
+    double dt, gamma;
+    int stage;              // 1, 2, 3; 0 = ghost fill only (copy of Wc)
+};
+
+// RK coefficients of runge_kutta_3 (range_kutta.cpp:55, 69, 83) with the
+// reference's rounding (no contraction).
+__device__ __forceinline__ double rk_combine(int stage, double u0, double u, double r, double dt) {
+    if (stage == 1) return __dadd_rn(u0, __dmul_rn(dt, r));
+    if (stage == 2) return __dadd_rn(__dmul_rn(0.75, u0), __dmul_rn(0.25, __dadd_rn(u, __dmul_rn(dt, r))));
+    return __dadd_rn(__dmul_rn(1.0 / 3.0, u0), __dmul_rn(2.0 / 3.0, __dadd_rn(u, __dmul_rn(dt, r))));
+}
+
+__global__ void __launch_bounds__(256) stage_kernel64(StageArgs64 a) {
+    const Layout &L = a.L;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    int c[3] = {i, j, k};
+    int flip;
+    const int kind = resolve_source(L, a.b, c, flip);
+    double W[5];
+    if (kind != SRC_CELL) {
+        special_state(kind, W);
+    } else {
+        const long s = L.at(c[0], c[1], c[2]);
+        if (a.stage == 0) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) W[q] = a.Wc[q][s];
+            if (W[0] <= 0.0) W[0] = 1e-12;
+        } else {
+            double U0[5], U[5];
+            p2c_exact(a.W0[0][s], a.W0[1][s], a.W0[2][s], a.W0[3][s], a.W0[4][s], a.gamma, U0);
+            if (a.stage == 1) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) U[q] = U0[q];
+            } else {
+                p2c_exact(a.Wc[0][s], a.Wc[1][s], a.Wc[2][s], a.Wc[3][s], a.Wc[4][s], a.gamma, U);
+            }
+            const bool inner = is_interior(L, c);
+            double Un[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const double r = inner ? a.Rhs[q][s] : 0.0;
+                Un[q] = rk_combine(a.stage, U0[q], U[q], r, a.dt);
+            }
+            c2p_exact(Un, a.gamma, W);
+        }
+    }
+    apply_flips(flip, W);
+    const long o = L.at(i, j, k);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) a.Wout[q][o] = W[q];
+}
+
+// --------------------------------------------------------------- mixed path
+
+struct StageArgsMixed {
+    const double *U0[5];    // step-start conserved state (FP64)
+    const double *Uc[5];    // current stage conserved state (FP64)
+    const float *Rhs[5];    // FP32 right-hand side
+    double *Uout[5];        // next conserved state (FP64)
+    float *Wout[5];         // FP32 primitives for the stencil kernels
+    Layout L;               // FP64 layout
+    Layout L32;             // FP32 layout
+    BcInfo b;
+    double dt, gamma;
+    int stage;              // 1, 2, 3; 0 = ghost fill only
+};
+
+__global__ void __launch_bounds__(256) stage_kernel_mixed(StageArgsMixed a) {
+    const Layout &L = a.L;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    int c[3] = {i, j, k};
+    int flip;
+    const int kind = resolve_source(L, a.b, c, flip);
+    double U[5], W[5];
+    if (kind != SRC_CELL) {
+        special_state(kind, W);
+        apply_flips(flip, W);
+        p2c_exact(W[0], W[1], W[2], W[3], W[4], a.gamma, U);
+    } else {
+        const long s = L.at(c[0], c[1], c[2]);
+        if (a.stage == 0) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) U[q] = a.Uc[q][s];
+        } else {
+            const bool inner = is_interior(L, c);
+            const long s32 = a.L32.at(c[0], c[1], c[2]);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const double r = inner ? (double)a.Rhs[q][s32] : 0.0;
+                const double u0 = a.U0[q][s];
+                const double u = a.stage == 1 ? u0 : a.Uc[q][s];
+                U[q] = a.stage == 1 ? u0 + a.dt * r
+                     : a.stage == 2 ? 0.75 * u0 + 0.25 * (u + a.dt * r)
+                                    : (1.0 / 3.0) * u0 + (2.0 / 3.0) * (u + a.dt * r);
+            }
+        }
+        if (U[0] <= 0.0) U[0] = 1e-12;
+        if (flip & 1) U[1] = -U[1];
+        if (flip & 2) U[2] = -U[2];
+        if (flip & 4) U[3] = -U[3];
+        c2p_exact(U, a.gamma, W);  // FP64 pressure recovery
+    }
+    const long o = L.at(i, j, k);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) a.Uout[q][o] = U[q];
+    const long o32 = a.L32.at(i, j, k);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) a.Wout[q][o32] = (float)W[q];
+}
+
+// --------------------------------------------------------------- reductions
+
+// Reduction kernels write one partial per block; a single-block kernel then
+// combines the partials in a fixed order, so results are deterministic.
+constexpr int RED_THREADS = 256;
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double v[NV], double *partial_out) {
+    __shared__ double sh[NV][RED_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double x = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[q][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = 0.0;
+            for (int w = 0; w < RED_THREADS / 32; ++w) s += sh[q][w];
+            partial_out[q] = s;
+        }
+    }
+}
+
+__device__ __forceinline__ double block_min(double x, double *partial_out) {
+    __shared__ double sh[RED_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_down_sync(0xffffffffu, x, o));
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = sh[0];
+        for (int w = 1; w < RED_THREADS / 32; ++w) m = fmin(m, sh[w]);
+        *partial_out = m;
+    }
+    return x;
+}
+
+// Per-cell CFL bound of compute_timestep (timestep.cpp:12-20) from the FP64
+// conserved state: u = rhou/rho, p = (gamma-1)(E - 0.5 rho u^2) (v, w are not
+// used), a = sqrt(gamma p / rho), bound = dx / (|u| + a).
+__device__ __forceinline__ double cfl_bound(const double U[5], double gamma, double dx) {
+    double rho = U[0];
+    double u = U[1] / rho;
+    double p = __dmul_rn(gamma - 1., __dsub_rn(U[4], __dmul_rn(__dmul_rn(__dmul_rn(0.5, rho), u), u)));
+    double a = sqrt(__dmul_rn(gamma, p) / rho);
+    return dx / __dadd_rn(fabs(u), a);
+}
+
+}  // namespace ns3d

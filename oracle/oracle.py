@@ -184,3 +184,49 @@ class RefSolver(_Base):
     def timestep(self) -> float: return self.lib.ref_timestep()
     def total_energy(self) -> float: return self.lib.ref_total_energy()
     def time_advance(self): self.lib.ref_time_advance()
+
+
+def _kat_lib(path):
+    lib = C.CDLL(path)
+    pre = "ref_" if path == REF_LIB else "orc_"
+    f_weno = getattr(lib, pre + "weno5")
+    f_weno.restype = C.c_double
+    f_weno.argtypes = [_dp]
+    f_lin = getattr(lib, pre + "mdcd_linear")
+    f_lin.restype = C.c_double
+    f_lin.argtypes = [_dp, C.c_double, C.c_double]
+    f_hyb = getattr(lib, pre + "mdcd_hybrid")
+    f_hyb.restype = C.c_double
+    f_hyb.argtypes = [_dp, C.c_double, C.c_double]
+    f_rie = getattr(lib, pre + "riemann")
+    f_rie.restype = None
+    f_rie.argtypes = [C.c_int, _dp, _dp, C.c_int, C.c_double, _dp]
+    return f_weno, f_lin, f_hyb, f_rie
+
+
+class Kernels:
+    """Scalar interpolation / Riemann kernels of one oracle (port or reference)."""
+
+    def __init__(self, which: str = "port"):
+        if which == "port" and not os.path.exists(PORT_LIB):
+            build(ref=False)
+        self._w, self._l, self._h, self._r = _kat_lib(PORT_LIB if which == "port" else REF_LIB)
+
+    def weno5(self, f):
+        a = np.ascontiguousarray(f, dtype=np.float64)
+        return self._w(_ptr(a))
+
+    def mdcd_linear(self, f, disp, diss):
+        a = np.ascontiguousarray(f, dtype=np.float64)
+        return self._l(_ptr(a), disp, diss)
+
+    def mdcd_hybrid(self, f, disp, diss):
+        a = np.ascontiguousarray(f, dtype=np.float64)
+        return self._h(_ptr(a), disp, diss)
+
+    def riemann(self, solver, UL, UR, direction, gamma):
+        a = np.ascontiguousarray(UL, dtype=np.float64)
+        b = np.ascontiguousarray(UR, dtype=np.float64)
+        out = np.zeros(5)
+        self._r(int(solver), _ptr(a), _ptr(b), int(direction), float(gamma), _ptr(out))
+        return out

@@ -175,3 +175,45 @@ double ref_total_energy(void) {
 void ref_time_advance(void) { time_advance(S->F, S->C, S->G, S->P); }
 
 }  // extern "C"
+
+/* ---- per-function known-answer wrappers around the reference's free
+ * functions (ns3d_func.h:77-112), used to generate the scalar KAT fixtures. */
+extern "C" {
+
+double ref_weno5(const double *f) {
+    std::array<double, 6> a;
+    for (int i = 0; i < 6; ++i) a[i] = f[i];
+    return weno5_interpolate(a);
+}
+
+double ref_mdcd_linear(const double *f, double disp, double diss) {
+    std::array<double, 6> a;
+    for (int i = 0; i < 6; ++i) a[i] = f[i];
+    SolverParams P;
+    P.mdcd_disp = disp; P.mdcd_diss = diss;
+    return mdcd_linear_interpolate(a, P);
+}
+
+double ref_mdcd_hybrid(const double *f, double disp, double diss) {
+    std::array<double, 6> a;
+    for (int i = 0; i < 6; ++i) a[i] = f[i];
+    SolverParams P;
+    P.mdcd_disp = disp; P.mdcd_diss = diss;
+    return mdcd_hybrid_interpolate(a, P);
+}
+
+void ref_riemann(int solver, const double *UL, const double *UR, int dir, double gamma, double *F) {
+    std::vector<double> L(UL, UL + 5), R(UR, UR + 5), out(5, 0.0);
+    double nx = dir == 0, ny = dir == 1, nz = dir == 2;
+    switch (solver) {
+        case 0: Roe_Riemann_solver(out, L, R, nx, ny, nz, gamma); break;
+        case 1: Rusanov_Riemann_solver(out, L, R, nx, ny, nz, gamma); break;
+        case 2: HLLC_Riemann_solver(out, L, R, nx, ny, nz, gamma); break;
+        case 3: HLL_Riemann_solver(out, L, R, nx, ny, nz, gamma); break;
+        case 4: HLLC_p_Riemann_solver(out, L, R, nx, ny, nz, gamma); break;
+        case 5: AUSM_Riemann_solver(out, L, R, nx, ny, nz, gamma); break;
+    }
+    for (int i = 0; i < 5; ++i) F[i] = out[i];
+}
+
+}  // extern "C"
