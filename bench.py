@@ -275,9 +275,12 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    tpath = os.path.join(ROOT, "profiles", f"traffic_{n}.txt")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(dom)
+        for ln in open(tpath):
+            f = ln.split()
+            if len(f) == 2 and not ln.startswith("#") and f[0] == dom:
+                traffic = float(f[1])
 
     # end to end through the C ABI with host buffers (pinned)
     e2e = None
