@@ -38,8 +38,8 @@ __global__ void __launch_bounds__(RED_THREADS) diag_kernel(ViscArgs<R> a, double
 #pragma unroll
         for (int q = 0; q < 9; ++q) s += (double)g[q] * (double)g[q];
         acc[1] += s;
-        const double T = (double)a.W[4][c] / ((double)a.W[0][c] * (double)a.Rgas);
-        acc[2] += (double)a.mu0 * pow(T, 1.5) * (1.0 + (double)a.S) / (T + (double)a.S);
+        const double T = (double)a.T[c];
+        acc[2] += sutherland((double)a.mu0, (double)a.S, T);
         acc[3] += rho;
         acc[4] += u * u + v * v + w * w;
     }
@@ -159,6 +159,15 @@ __global__ void derive_kernel_mixed(const double *const *Up, double *const *Out,
     }
 }
 
+// T = p/(rho Rgas) of every cell (after a full-field upload).
+__global__ void temp_kernel64(const double *const *Wp, double *T, Layout L, double Rgas) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    const long c = L.at(i, j, k);
+    const double rr = Wp[0][c] <= 0.0 ? 1e-12 : Wp[0][c];
+    T[c] = Wp[4][c] / __dmul_rn(rr, Rgas);
+}
+
 template <typename T>
 __global__ void widen_kernel(const T *src, double *dst, Layout Ls, Layout Ld) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
@@ -192,8 +201,10 @@ struct ns3d_handle {
     double *S[3][5] = {};
     int s0 = 0;          // buffer holding the current state
     double *rhs64[5] = {};
+    double *T64 = nullptr;
     float *w32[5] = {};
     float *rhs32[5] = {};
+    float *T32 = nullptr;
     void *visc[9] = {};  // double (plain) or float (mixed), interior layout
     double *scratch[5] = {};   // download staging (points into a state buffer)
     double **dptr = nullptr;   // device array of pointer tables
@@ -279,8 +290,13 @@ SweepArgs<R> sweep_args(ns3d_handle *h, int dir) {
     a.outflow_lo = h->P.bc[2 * dir] == NS3D_OUTFLOW;
     a.outflow_hi = h->P.bc[2 * dir + 1] == NS3D_OUTFLOW;
     a.inv_h = (R)(dir == 0 ? h->ph.inv_dx : dir == 1 ? h->ph.inv_dy : h->ph.inv_dz);
+    a.h = (R)(dir == 0 ? h->ph.dx : dir == 1 ? h->ph.dy : h->ph.dz);
     if constexpr (sizeof(R) == 8) a.sp = h->sp64; else a.sp = h->sp32;
     a.first = dir == 0;
+    a.visc = h->ph.mu != 0.0;
+    // node fluxes of this direction for rhou, rhov, rhow, E: F_v, H_v, G_v
+    static const int comp[3][4] = {{0, 3, 4, 6}, {3, 1, 5, 7}, {4, 5, 2, 8}};
+    for (int q = 0; q < 4; ++q) a.V[q] = (const R *)h->visc[comp[dir][q]];
     return a;
 }
 
@@ -288,15 +304,15 @@ template <typename R>
 ViscArgs<R> visc_args(ns3d_handle *h) {
     ViscArgs<R> a;
     for (int q = 0; q < 5; ++q) {
-        if constexpr (sizeof(R) == 8) { a.W[q] = h->S[h->s0][q]; a.Rhs[q] = h->rhs64[q]; }
-        else { a.W[q] = h->w32[q]; a.Rhs[q] = h->rhs32[q]; }
+        if constexpr (sizeof(R) == 8) a.W[q] = h->S[h->s0][q];
+        else a.W[q] = h->w32[q];
     }
     for (int q = 0; q < 9; ++q) a.V[q] = (R *)h->visc[q];
+    if constexpr (sizeof(R) == 8) a.T = h->T64; else a.T = h->T32;
     a.L = sizeof(R) == 8 ? h->L64 : h->L32;
     for (int d = 0; d < 3; ++d) a.periodic[d] = h->bc.periodic[d];
     a.h[0] = (R)h->ph.dx; a.h[1] = (R)h->ph.dy; a.h[2] = (R)h->ph.dz;
-    a.inv_h[0] = (R)h->ph.inv_dx; a.inv_h[1] = (R)h->ph.inv_dy; a.inv_h[2] = (R)h->ph.inv_dz;
-    a.Rgas = (R)h->ph.Rgas; a.mu0 = (R)h->ph.mu; a.S = (R)h->ph.S;
+    a.mu0 = (R)h->ph.mu; a.S = (R)h->ph.S;
     a.cp_over_pr = (R)(h->ph.Cp / h->ph.Pr);
     return a;
 }
@@ -305,6 +321,15 @@ template <typename R>
 int rhs_impl(ns3d_handle *h) {
     cudaStream_t st = h->stream;
     cudaError_t e;
+    if (h->ph.mu != 0.0) {  // Re = inf: the viscous terms are exactly zero
+        ViscArgs<R> va = visc_args<R>(h);
+        dim3 g((va.L.nx + VTX - 1) / VTX, (va.L.ny + VTY - 1) / VTY, va.L.nz);
+        prof_begin(h, "viscous_flux");
+        viscous_flux_kernel<R><<<g, dim3(VTX, VTY), 0, st>>>(va);
+        prof_end(h);
+        h->launches += 1;
+        CK(h, cudaGetLastError(), "viscous kernel");
+    }
     prof_begin(h, "sweep_x");
     e = sweep_x(sweep_args<R>(h, 0), st); if (e != cudaSuccess) return cuda_fail(h, e, "sweep_x");
     prof_end(h);
@@ -315,18 +340,6 @@ int rhs_impl(ns3d_handle *h) {
     e = sweep_z(sweep_args<R>(h, 2), st); if (e != cudaSuccess) return cuda_fail(h, e, "sweep_z");
     prof_end(h);
     h->launches += 3;
-    if (h->ph.mu != 0.0) {  // Re = inf: the viscous terms are exactly zero
-        ViscArgs<R> va = visc_args<R>(h);
-        dim3 g = cell_grid(va.L, false, 128);
-        prof_begin(h, "viscous_flux");
-        viscous_flux_kernel<R><<<g, 128, 0, st>>>(va);
-        prof_end(h);
-        prof_begin(h, "viscous_div");
-        viscous_div_kernel<R><<<g, 128, 0, st>>>(va);
-        prof_end(h);
-        h->launches += 2;
-        CK(h, cudaGetLastError(), "viscous kernels");
-    }
     return NS3D_OK;
 }
 
@@ -344,6 +357,7 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
             a.W0[q] = h->S[src0][q]; a.Wc[q] = h->S[srcc][q]; a.Rhs[q] = h->rhs64[q]; a.Wout[q] = h->S[dst][q];
         }
         a.L = h->L64; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
+        a.Tout = h->T64; a.Rgas = h->ph.Rgas;
         prof_begin(h, "stage");
         stage_kernel64<<<g, 128, 0, st>>>(a);
         prof_end(h);
@@ -354,6 +368,7 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
             a.Uout[q] = h->S[dst][q]; a.Wout[q] = h->w32[q];
         }
         a.L = h->L64; a.L32 = h->L32; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
+        a.Tout = h->T32; a.Rgas = h->ph.Rgas;
         prof_begin(h, "stage");
         stage_kernel_mixed<<<g, 128, 0, st>>>(a);
         prof_end(h);
@@ -520,7 +535,7 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
     h->red_blocks = dev_sms * 4;
     size_t bytes = 15 * p64;                                   // three state buffers
-    bytes += h->mixed ? 10 * p32 : 5 * p64;                    // (w32 + rhs32) or rhs64
+    bytes += h->mixed ? 11 * p32 : 6 * p64;                    // (w32 + rhs32 + T32) or (rhs64 + T64)
     bytes += 9 * vis_elems * (h->mixed ? 4 : 8);               // viscous node fluxes
     bytes += 256 * 32;                                         // pointer tables
     bytes += ((size_t)h->red_blocks * 8 * 8 + 255) / 256 * 256;  // partials
@@ -534,8 +549,10 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     if (h->mixed) {
         for (int q = 0; q < 5; ++q) { h->w32[q] = (float *)p; p += p32; }
         for (int q = 0; q < 5; ++q) { h->rhs32[q] = (float *)p; p += p32; }
+        h->T32 = (float *)p; p += p32;
     } else {
         for (int q = 0; q < 5; ++q) { h->rhs64[q] = (double *)p; p += p64; }
+        h->T64 = (double *)p; p += p64;
     }
     for (int q = 0; q < 9; ++q) { h->visc[q] = p; p += vis_elems * (h->mixed ? 4 : 8); }
     h->dptr = (double **)p; p += 256 * 32;
@@ -627,8 +644,8 @@ static int download_plane(ns3d_handle *h, double *dst, const double *src) {
 // FP64 primitives of the full field sit in buffer b.  Plain path: b becomes
 // the state (after the ghost fill when apply_bc).  Mixed path: FP64
 // conserved state + FP32 primitives are derived from it.
-__global__ void upload_mixed_kernel(const double *const *Wp, double *const *Up, float *const *W32, Layout L,
-                                    Layout L32, double gamma) {
+__global__ void upload_mixed_kernel(const double *const *Wp, double *const *Up, float *const *W32, float *T32,
+                                    Layout L, Layout L32, double gamma, double Rgas) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
     if (i >= L.sx) return;
     const long c = L.at(i, j, k), c32 = L32.at(i, j, k);
@@ -638,20 +655,29 @@ __global__ void upload_mixed_kernel(const double *const *Wp, double *const *Up, 
     c2p_exact(U, gamma, W);
 #pragma unroll
     for (int q = 0; q < 5; ++q) { Up[q][c] = U[q]; W32[q][c32] = (float)W[q]; }
+    T32[c32] = (float)(W[4] / (W[0] * Rgas));
 }
 
 static int finish_upload(ns3d_handle *h, int b, bool apply_bc) {
     const int dst = (b + 1) % 3, dst2 = (b + 2) % 3;
     int r;
     if (!h->mixed) {
-        if (!apply_bc) { h->s0 = b; return NS3D_OK; }
+        if (!apply_bc) {
+            dim3 g = cell_grid(h->L64, true, 128);
+            temp_kernel64<<<g, 128, 0, h->stream>>>(state_table(h, b), h->T64, h->L64, h->ph.Rgas);
+            h->launches += 1;
+            CK(h, cudaGetLastError(), "temperature");
+            h->s0 = b;
+            return NS3D_OK;
+        }
         if ((r = stage_async(h, 0, b, b, dst, 0.0))) return r;
         h->s0 = dst;
         return NS3D_OK;
     }
     dim3 g = cell_grid(h->L64, true, 128);
     upload_mixed_kernel<<<g, 128, 0, h->stream>>>(state_table(h, b), state_table(h, dst),
-                                                  (float *const *)(h->dptr + 25), h->L64, h->L32, h->ph.gamma);
+                                                  (float *const *)(h->dptr + 25), h->T32, h->L64, h->L32,
+                                                  h->ph.gamma, h->ph.Rgas);
     h->launches += 1;
     CK(h, cudaGetLastError(), "upload conversion");
     h->s0 = dst;
@@ -834,8 +860,13 @@ int ns3d_diagnostics(ns3d_handle *h, double out[6]) {
         dim3 g = cell_grid(h->L64, true, 128);
         derive_kernel_mixed<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), state_table(h, b), h->L64, h->ph.gamma,
                                                        h->ph.Rgas, NS3D_PRIMITIVE);
+        const int bt = (h->s0 + 2) % 3;
+        derive_kernel_mixed<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), state_table(h, bt), h->L64, h->ph.gamma,
+                                                       h->ph.Rgas, NS3D_TEMPERATURE);
+        h->launches += 1;
         ViscArgs<double> a = visc_args<double>(h);
         for (int q = 0; q < 5; ++q) a.W[q] = h->S[b][q];
+        a.T = h->S[bt][0];
         a.L = h->L64;
         diag_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(a, vol, h->partials);
         h->launches += 1;

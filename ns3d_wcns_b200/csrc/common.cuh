@@ -82,3 +82,19 @@ __device__ __forceinline__ void p2c_f(float r, float u, float v, float w, float 
 }
 
 }  // namespace ns3d
+
+namespace ns3d {
+// Asynchronous global -> shared copies (LDGSTS), used to stage the next chunk
+// of a sweep while the current one computes.
+__device__ __forceinline__ void cp_async(double *smem_dst, const double *gsrc) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async(float *smem_dst, const float *gsrc) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+}  // namespace ns3d

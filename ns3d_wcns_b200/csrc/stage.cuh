@@ -80,9 +80,10 @@ struct StageArgs64 {
     const double *Wc[5];    // current stage state
     const double *Rhs[5];
     double *Wout[5];
+    double *Tout;           // T = p/(rho Rgas) of the new state (field_structures.h:486)
     Layout L;
     BcInfo b;
-    double dt, gamma;
+    double dt, gamma, Rgas;
     int stage;              // 1, 2, 3; 0 = ghost fill only (copy of Wc)
 };
 
@@ -134,6 +135,7 @@ __global__ void __launch_bounds__(256) stage_kernel64(StageArgs64 a) {
     const long o = L.at(i, j, k);
 #pragma unroll
     for (int q = 0; q < 5; ++q) a.Wout[q][o] = W[q];
+    a.Tout[o] = W[4] / __dmul_rn(W[0], a.Rgas);
 }
 
 // --------------------------------------------------------------- mixed path
@@ -144,10 +146,11 @@ struct StageArgsMixed {
     const float *Rhs[5];    // FP32 right-hand side
     double *Uout[5];        // next conserved state (FP64)
     float *Wout[5];         // FP32 primitives for the stencil kernels
+    float *Tout;            // FP32 temperature
     Layout L;               // FP64 layout
     Layout L32;             // FP32 layout
     BcInfo b;
-    double dt, gamma;
+    double dt, gamma, Rgas;
     int stage;              // 1, 2, 3; 0 = ghost fill only
 };
 
@@ -194,6 +197,7 @@ __global__ void __launch_bounds__(256) stage_kernel_mixed(StageArgsMixed a) {
     const long o32 = a.L32.at(i, j, k);
 #pragma unroll
     for (int q = 0; q < 5; ++q) a.Wout[q][o32] = (float)W[q];
+    a.Tout[o32] = (float)(W[4] / (W[0] * a.Rgas));
 }
 
 // --------------------------------------------------------------- reductions

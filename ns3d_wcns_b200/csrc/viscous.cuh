@@ -1,16 +1,22 @@
-// viscous.cuh -- viscous terms of the RHS.
+// viscous.cuh -- node viscous fluxes.
 //
-// Kernel 1 (viscous_flux_kernel): at every interior node, the 12 derivatives
-// of u, v, w, T with the order chosen by distance to a non-periodic boundary
+// viscous_flux_kernel: at every interior node, the 12 derivatives of u, v, w, T
+// with the order chosen by distance to a non-periodic boundary
 // (compute_gradients + choose_scheme, ViscousFlux.cpp:15-148), Sutherland mu
 // (field_structures.h:96-106), stresses and heat flux, stored as the nine
 // distinct node fluxes txx tyy tzz txy txz tyz ex ey ez
 // (compute_viscous_flux, ViscousFlux.cpp:151-208; F_v = (txx,txy,txz,ex),
 // H_v = (txy,tyy,tyz,ey), G_v = (txz,tyz,tzz,ez)).
 //
-// Kernel 2 (viscous_div_kernel): rhs += D_x F_v + D_y H_v + D_z G_v with the
-// same boundary orders (compute_vis_flux, ViscousFlux.cpp:210-255).  In
-// periodic directions the stencil wraps to the interior node, which is what
+// A block owns a 32 x 8 tile of one z-plane: the tile and its 3-cell x/y halo
+// of (u, v, w, T) are staged in shared memory, x and y derivatives read the
+// tile, z derivatives read the neighbouring planes from global memory
+// (coalesced rows).  T is the array the stage kernel stores (p/(rho Rgas)).
+//
+// The divergence of these fluxes (compute_vis_flux, ViscousFlux.cpp:210-255)
+// is added by the three sweeps, each differencing its direction's fluxes
+// along the lines it already stages (sweep.cuh).  In periodic directions that
+// stencil wraps to the interior node, which is what
 // exchange_halos_viscous_flux (field_structures.h:877-932) copies into the
 // ghosts; in non-periodic directions the orders keep the stencil inside.
 #pragma once
@@ -22,13 +28,12 @@ namespace ns3d {
 template <typename R>
 struct ViscArgs {
     const R *W[5];          // primitives (padded layout)
-    R *Rhs[5];              // RHS (padded layout)
-    R *V[9];                // node fluxes, interior-only layout (k*ny + j)*nx + i
+    const R *T;             // temperature (padded layout)
+    R *V[9];                // node fluxes, interior layout (k*ny + j)*nx + i
     Layout L;
     int periodic[3];
-    R inv_h[3];             // 1/(2h), 1/(12h), 1/(60h) are formed from these
     R h[3];
-    R Rgas, mu0, S, cp_over_pr;
+    R mu0, S, cp_over_pr;
 };
 
 // choose_scheme, ViscousFlux.cpp:33-50 (idx relative to the first interior node)
@@ -52,53 +57,58 @@ __device__ __forceinline__ R dstencil(F f, int order, R h) {
     return (f(3) - R(9) * f(2) + R(45) * f(1) - R(45) * f(-1) + R(9) * f(-2) - f(-3)) / (R(60) * h);
 }
 
+// Sutherland's law mu0 T^1.5 (1+S)/(T+S), with T^1.5 evaluated as T sqrt(T).
 template <typename R>
-__device__ __forceinline__ R temp_at(const ViscArgs<R> &a, long id) {
-    return a.W[4][id] / (a.W[0][id] * a.Rgas);  // T = p/(rho Rgas), field_structures.h:486
+__device__ __forceinline__ R sutherland(R mu0, R S, R T) {
+    return mu0 * (T * sqrt(T)) * (R(1) + S) / (T + S);
 }
 
-// All 12 derivatives at interior node (i,j,k) (ghost-inclusive indices).
+constexpr int VTX = 32, VTY = 8, VH = NG;
+
 template <typename R>
-__device__ __forceinline__ void node_gradients(const ViscArgs<R> &a, int i, int j, int k, R g[12]) {
+__global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a) {
+    __shared__ R sm[4][VTY + 2 * VH][VTX + 2 * VH];
     const Layout &L = a.L;
-    const int o[3] = {visc_order(i - NG, L.nx, a.periodic[0]), visc_order(j - NG, L.ny, a.periodic[1]),
-                      visc_order(k - NG, L.nz, a.periodic[2])};
-    const long stride[3] = {1, (long)L.px, (long)L.px * L.sy};
-    const long c = L.at(i, j, k);
+    const int x0 = blockIdx.x * VTX, y0 = blockIdx.y * VTY, k = blockIdx.z + NG;
+    const R *src[4] = {a.W[1], a.W[2], a.W[3], a.T};
+    // tile + halo: ghost-inclusive coordinates (x0 + tx, y0 + ty)
+    for (int t = threadIdx.y * VTX + threadIdx.x; t < (VTX + 2 * VH) * (VTY + 2 * VH); t += VTX * VTY) {
+        const int tx = t % (VTX + 2 * VH), ty = t / (VTX + 2 * VH);
+        const int gx = x0 + tx, gy = y0 + ty;
+        if (gx < L.sx && gy < L.sy) {
+            const long id = L.at(gx, gy, k);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const long s = stride[d];
-        const R h = a.h[d];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            const R *f = a.W[1 + q];
-            g[3 * q + d] = dstencil<R>([&](int off) { return f[c + off * s]; }, o[d], h);
+            for (int q = 0; q < 4; ++q) sm[q][ty][tx] = src[q][id];
         }
-        g[9 + d] = dstencil<R>([&](int off) { return temp_at(a, c + off * s); }, o[d], h);
     }
-}
-
-template <typename R>
-__global__ void __launch_bounds__(256) viscous_flux_kernel(ViscArgs<R> a) {
-    const Layout &L = a.L;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    if (i >= L.nx) return;
-    R g[12];
-    node_gradients(a, i + NG, j + NG, k + NG, g);
-    const long c = L.at(i + NG, j + NG, k + NG);
-    const R T = temp_at(a, c);
-    // SolverParams::get_mu, field_structures.h:96-106
-    const R mu = a.mu0 * pow(T, R(1.5)) * (R(1) + a.S) / (T + a.S);
-    const R ux = g[0], uy = g[1], uz = g[2], vx = g[3], vy = g[4], vz = g[5];
-    const R wx = g[6], wy = g[7], wz = g[8], Tx = g[9], Ty = g[10], Tz = g[11];
+    __syncthreads();
+    const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
+    if (i >= L.nx || j >= L.ny) return;
+    const int ox = visc_order(i, L.nx, a.periodic[0]);
+    const int oy = visc_order(j, L.ny, a.periodic[1]);
+    const int oz = visc_order(k - NG, L.nz, a.periodic[2]);
+    const int cx = threadIdx.x + VH, cy = threadIdx.y + VH;
+    const long c = L.at(i + NG, j + NG, k);
+    const long zs = (long)L.px * L.sy;
+    R g[4][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        g[q][0] = dstencil<R>([&](int o) { return sm[q][cy][cx + o]; }, ox, a.h[0]);
+        g[q][1] = dstencil<R>([&](int o) { return sm[q][cy + o][cx]; }, oy, a.h[1]);
+        const R *f = src[q];
+        g[q][2] = dstencil<R>([&](int o) { return f[c + o * zs]; }, oz, a.h[2]);
+    }
+    const R T = sm[3][cy][cx];
+    const R mu = sutherland(a.mu0, a.S, T);
+    const R ux = g[0][0], uy = g[0][1], uz = g[0][2], vx = g[1][0], vy = g[1][1], vz = g[1][2];
+    const R wx = g[2][0], wy = g[2][1], wz = g[2][2], Tx = g[3][0], Ty = g[3][1], Tz = g[3][2];
     const R div = ux + vy + wz;
     const R m2 = R(2) * mu, m23 = R(2.0 / 3.0) * mu * div;
     const R txx = m2 * ux - m23, tyy = m2 * vy - m23, tzz = m2 * wz - m23;
     const R txy = mu * (uy + vx), txz = mu * (uz + wx), tyz = mu * (vz + wy);
     const R kq = mu * a.cp_over_pr;
-    const R u = a.W[1][c], v = a.W[2][c], w = a.W[3][c];
-    const long o = ((long)k * L.ny + j) * L.nx + i;
+    const R u = sm[0][cy][cx], v = sm[1][cy][cx], w = sm[2][cy][cx];
+    const long o = ((long)(k - NG) * L.ny + j) * L.nx + i;
     a.V[0][o] = txx; a.V[1][o] = tyy; a.V[2][o] = tzz;
     a.V[3][o] = txy; a.V[4][o] = txz; a.V[5][o] = tyz;
     a.V[6][o] = u * txx + v * txy + w * txz + kq * Tx;
@@ -106,35 +116,25 @@ __global__ void __launch_bounds__(256) viscous_flux_kernel(ViscArgs<R> a) {
     a.V[8][o] = u * txz + v * tyz + w * tzz + kq * Tz;
 }
 
+// All 12 derivatives at interior node (i,j,k) (ghost-inclusive indices), for
+// the reductions.
 template <typename R>
-__global__ void __launch_bounds__(256) viscous_div_kernel(ViscArgs<R> a) {
+__device__ __forceinline__ void node_gradients(const ViscArgs<R> &a, int i, int j, int k, R g[12]) {
     const Layout &L = a.L;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    if (i >= L.nx) return;
-    const int n[3] = {L.nx, L.ny, L.nz};
-    const int p[3] = {i, j, k};
-    int o[3];
+    const int o[3] = {visc_order(i - NG, L.nx, a.periodic[0]), visc_order(j - NG, L.ny, a.periodic[1]),
+                      visc_order(k - NG, L.nz, a.periodic[2])};
+    const long stride[3] = {1, (long)L.px, (long)L.px * L.sy};
+    const long c = L.at(i, j, k);
+    const R *src[4] = {a.W[1], a.W[2], a.W[3], a.T};
 #pragma unroll
-    for (int d = 0; d < 3; ++d) o[d] = visc_order(p[d], n[d], a.periodic[d]);
-    // interior-layout index of the node shifted by off along d (wrapped if periodic)
-    auto at = [&](int d, int off) -> long {
-        int q[3] = {i, j, k};
-        int x = q[d] + off;
-        if (a.periodic[d]) { if (x < 0) x += n[d]; else if (x >= n[d]) x -= n[d]; }
-        q[d] = x;
-        return ((long)q[2] * L.ny + q[1]) * L.nx + q[0];
-    };
-    auto D = [&](int comp, int d) -> R {
-        const R *f = a.V[comp];
-        return dstencil<R>([&](int off) { return f[at(d, off)]; }, o[d], a.h[d]);
-    };
-    const long c = L.at(i + NG, j + NG, k + NG);
-    // momentum x: F_v momx = txx, H_v momx = txy, G_v momx = txz
-    R r = a.Rhs[1][c]; r += D(0, 0); r += D(3, 1); r += D(4, 2); a.Rhs[1][c] = r;
-    r = a.Rhs[2][c]; r += D(3, 0); r += D(1, 1); r += D(5, 2); a.Rhs[2][c] = r;
-    r = a.Rhs[3][c]; r += D(4, 0); r += D(5, 1); r += D(2, 2); a.Rhs[3][c] = r;
-    r = a.Rhs[4][c]; r += D(6, 0); r += D(7, 1); r += D(8, 2); a.Rhs[4][c] = r;
+    for (int d = 0; d < 3; ++d) {
+        const long s = stride[d];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const R *f = src[q];
+            g[3 * q + d] = dstencil<R>([&](int off) { return f[c + off * s]; }, o[d], a.h[d]);
+        }
+    }
 }
 
 }  // namespace ns3d

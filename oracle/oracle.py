@@ -22,6 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "_build", "libns3d_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libns3d_ref.so")
+DROPIN_LIB = os.path.join(HERE, "_ref", "libns3d_dropin.so")
 REF_SRC_DIR = "/root/reference"
 
 _dp = C.POINTER(C.c_double)
@@ -41,10 +42,16 @@ def build(ref: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     if ref and os.path.isdir(REF_SRC_DIR):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_DIR={REF_SRC_DIR}"], check=True)
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "ns3d_wcns_b200", "libns3d_b200.so")):
+            subprocess.run(["make", "-s", "-C", HERE, "dropin", f"REF_DIR={REF_SRC_DIR}"], check=True)
 
 
 def ref_available() -> bool:
     return os.path.exists(REF_LIB)
+
+
+def dropin_available() -> bool:
+    return os.path.exists(DROPIN_LIB)
 
 
 def _ptr(a: np.ndarray):
@@ -144,11 +151,11 @@ class PortSolver(_Base):
 class RefSolver(_Base):
     """The reference sources compiled in place (oracle/_ref/libns3d_ref.so)."""
 
-    def __init__(self, P, G, solver_in_text: Optional[str] = None):
+    def __init__(self, P, G, solver_in_text: Optional[str] = None, lib_path: str = REF_LIB):
         from ns3d_wcns_b200.config import format_solver_in
-        if not ref_available():
-            raise FileNotFoundError(REF_LIB)
-        lib = C.CDLL(REF_LIB)
+        if not os.path.exists(lib_path):
+            raise FileNotFoundError(lib_path)
+        lib = C.CDLL(lib_path)
         lib.ref_init_file.argtypes = [C.c_char_p, C.c_double]
         lib.ref_get.argtypes = [C.c_char_p, _dp, C.c_long]
         lib.ref_set.argtypes = [C.c_char_p, _dp, C.c_long]
