@@ -1,0 +1,61 @@
+// reduce.cuh -- block reductions for the global scalars (CFL time step,
+// kinetic energy, dissipation) and the per-cell CFL bound.
+#pragma once
+
+#include "common.cuh"
+
+namespace ns3d {
+
+// Reduction kernels write one partial per block; a single-block kernel then
+// combines the partials in a fixed order, so results are deterministic.
+constexpr int RED_THREADS = 256;
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double v[NV], double *partial_out) {
+    __shared__ double sh[NV][RED_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double x = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[q][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = 0.0;
+            for (int w = 0; w < RED_THREADS / 32; ++w) s += sh[q][w];
+            partial_out[q] = s;
+        }
+    }
+}
+
+__device__ __forceinline__ double block_min(double x, double *partial_out) {
+    __shared__ double sh[RED_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_down_sync(0xffffffffu, x, o));
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = sh[0];
+        for (int w = 1; w < RED_THREADS / 32; ++w) m = fmin(m, sh[w]);
+        *partial_out = m;
+    }
+    return x;
+}
+
+// Per-cell CFL bound of compute_timestep (timestep.cpp:12-20) from the FP64
+// conserved state: u = rhou/rho, p = (gamma-1)(E - 0.5 rho u^2) (v, w are not
+// used), a = sqrt(gamma p / rho), bound = dx / (|u| + a).
+__device__ __forceinline__ double cfl_bound(const double U[5], double gamma, double dx) {
+    double rho = U[0];
+    double u = U[1] / rho;
+    double p = __dmul_rn(gamma - 1., __dsub_rn(U[4], __dmul_rn(__dmul_rn(__dmul_rn(0.5, rho), u), u)));
+    double a = sqrt(__dmul_rn(gamma, p) / rho);
+    return dx / __dadd_rn(fabs(u), a);
+}
+
+}  // namespace ns3d
