@@ -38,6 +38,7 @@ extern "C" {
 #define NS3D_ERR_STATE (-7)         /* call out of order (e.g. no state uploaded) */
 #define NS3D_ERR_DT (-8)            /* time step <= 1e-12 (maincycle.cpp:46-52) */
 #define NS3D_ERR_TIMEOUT (-9)       /* a bounded device wait expired */
+#define NS3D_ERR_SIZE (-10)         /* grid larger than an entry point's stated maximum */
 
 /* ------------------------------------------------------------ enumerations */
 /* Same numbering as the reference enums (field_structures.h:131-165). */
@@ -175,6 +176,31 @@ int ns3d_last_launch_count(const ns3d_handle *h, long *count);
  * "<name> <launches> <total milliseconds>". */
 int ns3d_profile(ns3d_handle *h, int enable);
 int ns3d_profile_report(ns3d_handle *h, char *buf, long len);
+
+/* ---------------------------------------- scratch-free CFL time step
+ * No counterpart in the reference.  For host codes that cannot let a library
+ * allocate device memory -- solvers that hand out every device byte from
+ * their own pre-sized pool, and codes that capture their time loop into a
+ * CUDA graph -- this computes what ns3d_compute_timestep computes
+ * (compute_timestep, timestep.cpp:5-23) without a handle and without calling
+ * cudaMalloc, cudaFree or any allocating routine.
+ *   d_fields  five caller-owned device arrays rho, u, v, w, p in the unpadded
+ *             Field3D layout (sx*sy*sz doubles, sx = nx+6, ...);
+ *   d_dt_out  caller-owned device double receiving cfl * min dx/(|u|+a);
+ *   stream    cudaStream_t as void* (NULL: the default stream); the call only
+ *             enqueues work and returns before the result is ready.
+ * Limit: nx*ny*nz <= NS3D_NOALLOC_MAX_CELLS (2^27, e.g. 512^3); larger grids
+ * return NS3D_ERR_SIZE.  Its scratch is one fixed 128 KB device array of
+ * per-block partials (NS3D_NOALLOC_MAX_BLOCKS doubles) that every GPU which
+ * loads the library holds until the process exits.  All calls share that
+ * array, so calls that overlap on a GPU (other streams or host threads) race
+ * on it: serialise them.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture. */
+#define NS3D_NOALLOC_MAX_BLOCKS 16384
+#define NS3D_NOALLOC_MAX_CELLS (16384L * 256 * 32)
+int ns3d_compute_timestep_noalloc(const double *const d_fields[5], int nx, int ny, int nz, double gamma,
+                                  double cfl, double dx, double *d_dt_out, void *stream);
 
 #ifdef __cplusplus
 }

@@ -17,7 +17,7 @@ NS3D_FP64, NS3D_MIXED = 0, 1
 
 STATUS = {0: "NS3D_OK", -1: "NS3D_ERR_INVALID_ARG", -2: "NS3D_ERR_CONFIG", -3: "NS3D_ERR_OOM",
           -4: "NS3D_ERR_CUDA", -5: "NS3D_ERR_NONFINITE", -6: "NS3D_ERR_NO_DEVICE", -7: "NS3D_ERR_STATE",
-          -8: "NS3D_ERR_DT", -9: "NS3D_ERR_TIMEOUT"}
+          -8: "NS3D_ERR_DT", -9: "NS3D_ERR_TIMEOUT", -10: "NS3D_ERR_SIZE"}
 
 # every entry point declared in include/ns3d_b200.h
 EXPORTS = [
@@ -26,7 +26,7 @@ EXPORTS = [
     "ns3d_apply_boundary", "ns3d_compute_rhs", "ns3d_rk3_step", "ns3d_rk3_steps",
     "ns3d_compute_timestep", "ns3d_total_energy", "ns3d_diagnostics", "ns3d_time_advance",
     "ns3d_device_fields", "ns3d_set_stream", "ns3d_synchronize", "ns3d_last_launch_count",
-    "ns3d_profile", "ns3d_profile_report",
+    "ns3d_profile", "ns3d_profile_report", "ns3d_compute_timestep_noalloc",
 ]
 
 
@@ -87,5 +87,7 @@ def load() -> C.CDLL:
     lib.ns3d_last_launch_count.argtypes = [h, C.POINTER(C.c_long)]
     lib.ns3d_profile.argtypes = [h, C.c_int]
     lib.ns3d_profile_report.argtypes = [h, C.c_char_p, C.c_long]
+    lib.ns3d_compute_timestep_noalloc.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_double,
+                                                  C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
