@@ -627,17 +627,34 @@ int ns3d_last_launch_count(const ns3d_handle *h, long *count) {
 }
 
 // host Field3D array (sx*sy*sz doubles) -> padded device array
-static int upload_plane(ns3d_handle *h, double *dst, const double *src) {
+// Host Field3D arrays move as one contiguous copy each (full link bandwidth;
+// a pitched 2-D copy of ~2 KB rows is several times slower) through a
+// contiguous device staging array, repacked on the device.
+__global__ void repack_kernel(const double *src, double *dst, Layout L, int to_padded) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    const long flat = ((long)k * L.sy + j) * L.sx + i;
+    if (to_padded) dst[L.at(i, j, k)] = src[flat];
+    else dst[flat] = src[L.at(i, j, k)];
+}
+
+static int upload_plane(ns3d_handle *h, double *dst, const double *src, double *staging) {
     const Layout &L = h->L64;
-    CK(h, cudaMemcpy2DAsync(dst + L.off, (size_t)L.px * 8, src, (size_t)L.sx * 8, (size_t)L.sx * 8,
-                            (size_t)L.sy * L.sz, cudaMemcpyHostToDevice, h->stream), "upload");
+    const size_t n = (size_t)L.sx * L.sy * L.sz;
+    CK(h, cudaMemcpyAsync(staging, src, n * 8, cudaMemcpyHostToDevice, h->stream), "upload");
+    repack_kernel<<<cell_grid(L, true, 128), 128, 0, h->stream>>>(staging, dst, L, 1);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "repack");
     return NS3D_OK;
 }
 
-static int download_plane(ns3d_handle *h, double *dst, const double *src) {
+static int download_plane(ns3d_handle *h, double *dst, const double *src, double *staging) {
     const Layout &L = h->L64;
-    CK(h, cudaMemcpy2DAsync(dst, (size_t)L.sx * 8, src + L.off, (size_t)L.px * 8, (size_t)L.sx * 8,
-                            (size_t)L.sy * L.sz, cudaMemcpyDeviceToHost, h->stream), "download");
+    const size_t n = (size_t)L.sx * L.sy * L.sz;
+    repack_kernel<<<cell_grid(L, true, 128), 128, 0, h->stream>>>(src, staging, L, 0);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "pack");
+    CK(h, cudaMemcpyAsync(dst, staging, n * 8, cudaMemcpyDeviceToHost, h->stream), "download");
     return NS3D_OK;
 }
 
@@ -693,7 +710,8 @@ int ns3d_upload_primitives(ns3d_handle *h, const double *const fields[5]) {
     int r = set_device(h); if (r) return r;
     h->launches = 0;
     const int b = (h->s0 + 1) % 3;
-    for (int q = 0; q < 5; ++q) if ((r = upload_plane(h, h->S[b][q], fields[q]))) return r;
+    const int stg = (h->s0 + 2) % 3;
+    for (int q = 0; q < 5; ++q) if ((r = upload_plane(h, h->S[b][q], fields[q], h->S[stg][q]))) return r;
     if ((r = finish_upload(h, b, false))) return r;
     CK(h, cudaStreamSynchronize(h->stream), "synchronize");
     h->has_state = true;
@@ -742,33 +760,33 @@ int ns3d_download(ns3d_handle *h, int what, double *const out[]) {
     if (!h->has_state && what != NS3D_RHS) return fail(h, NS3D_ERR_STATE, "no state uploaded");
     int r = set_device(h); if (r) return r;
     const Layout &L = h->L64;
-    const int free_b = (h->s0 + 1) % 3;
-    // scratch for derived groups: the free state buffer (its contents are dead between steps)
+    const int free_b = (h->s0 + 1) % 3, free2 = (h->s0 + 2) % 3;
+    // scratch for derived groups: the free state buffers (their contents are dead between steps)
     double *const *scr = state_table(h, free_b);
     dim3 g = cell_grid(L, true, 128);
     if (what == NS3D_RHS) {
         if (!h->mixed) {
-            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->rhs64[q]))) return r;
+            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->rhs64[q], h->S[free_b][q]))) return r;
         } else {
             for (int q = 0; q < 5; ++q)
                 widen_kernel<float><<<g, 128, 0, h->stream>>>(h->rhs32[q], h->S[free_b][q], h->L32, L);
-            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->S[free_b][q]))) return r;
+            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->S[free_b][q], h->S[free2][q]))) return r;
         }
     } else if (!h->mixed) {
         if (what == NS3D_PRIMITIVE) {
-            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->S[h->s0][q]))) return r;
+            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->S[h->s0][q], h->S[free_b][q]))) return r;
         } else {
             derive_kernel64<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), scr, L, h->ph.gamma, h->ph.Rgas, what);
             CK(h, cudaGetLastError(), "derive");
-            for (int q = 0; q < nq; ++q) if ((r = download_plane(h, out[q], h->S[free_b][q]))) return r;
+            for (int q = 0; q < nq; ++q) if ((r = download_plane(h, out[q], h->S[free_b][q], h->S[free2][q]))) return r;
         }
     } else {
         if (what == NS3D_CONSERVED) {
-            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->S[h->s0][q]))) return r;
+            for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->S[h->s0][q], h->S[free_b][q]))) return r;
         } else {
             derive_kernel_mixed<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), scr, L, h->ph.gamma, h->ph.Rgas, what);
             CK(h, cudaGetLastError(), "derive");
-            for (int q = 0; q < nq; ++q) if ((r = download_plane(h, out[q], h->S[free_b][q]))) return r;
+            for (int q = 0; q < nq; ++q) if ((r = download_plane(h, out[q], h->S[free_b][q], h->S[free2][q]))) return r;
         }
     }
     CK(h, cudaStreamSynchronize(h->stream), "synchronize");
