@@ -177,6 +177,48 @@ int ns3d_last_launch_count(const ns3d_handle *h, long *count);
 int ns3d_profile(ns3d_handle *h, int enable);
 int ns3d_profile_report(ns3d_handle *h, char *buf, long len);
 
+/* ------------------------------------------------------------- adjoint
+ * Hand-written reverse mode of the RHS and of the RK3 step (no counterpart in
+ * the reference).  Plain FP64 path, periodic boundaries, component-wise
+ * WENO5 / MDCD_LINEAR interpolation with the Roe, Rusanov or HLL flux; other
+ * configurations return NS3D_ERR_CONFIG.  The state differentiated is the
+ * interior conserved field (the c2p/p2c round trip is the identity).
+ * Host arrays are Field3D-sized (sx*sy*sz); only interior entries are read,
+ * ghost entries of outputs are zero. */
+
+/* ubar = (dR/dU)^T rbar at the current state (R = compute_rhs). */
+int ns3d_vjp_rhs(ns3d_handle *h, const double *const rbar[5], double *const ubar[5]);
+
+/* ubar = (dU^{n+1}/dU^n)^T ubar_next for one runge_kutta_3 step of size dt
+ * from the current state (the state is left unchanged). */
+int ns3d_vjp_rk3_step(ns3d_handle *h, double dt, const double *const ubar_next[5], double *const ubar[5]);
+
+/* J = compute_total_energy after nsteps fixed-dt RK3 steps from the current
+ * state, and dJ/d(u,v,w) of the initial velocity at fixed rho and p, by a
+ * forward pass that keeps a checkpoint every checkpoint_every steps and a
+ * backward pass that recomputes each segment's stage states.  grad: three
+ * host arrays of nx*ny*nz (x fastest).  stats (nullable): [0] forward ms,
+ * [1] backward ms (recompute + adjoint), [2] peak adjoint device bytes,
+ * [3] recomputed steps.  The handle's state is the initial one on return. */
+int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int checkpoint_every, double *J,
+                                double *const grad[3], double stats[4]);
+
+/* ------------------------------------------------- verification helpers
+ * Host evaluation (no device needed) of the code the adjoint kernels run,
+ * for finite-difference checks.  No counterpart in the reference.
+ * ns3d_debug_face_vjp: U30 = conserved stencil U[q][m] (q = rho..E, m = cells
+ * i-2..i+3), Fbar5 = adjoint of the face flux; out30 = dF/dU^T Fbar (same
+ * indexing); flux5 (nullable) = the production face flux of that stencil.
+ * interpolation: NS3D_WENO5 | NS3D_MDCD_LINEAR (lin = its six coefficients);
+ * riemann: NS3D_ROE | NS3D_RUSANOV | NS3D_HLL.
+ * ns3d_debug_visc_vjp: pointwise node viscous flux at x4 = (u,v,w,T) with
+ * gradients g12 (d{u,v,w,T}/d{x,y,z}); V9 (nullable) = the nine fluxes
+ * txx tyy tzz txy txz tyz ex ey ez, xb4/gb12 = their VJP with Vbar9. */
+int ns3d_debug_face_vjp(int direction, int interpolation, int riemann, double gamma, const double lin[6],
+                        const double *U30, const double *Fbar5, double *out30, double *flux5);
+int ns3d_debug_visc_vjp(double mu0, double S, double cp_over_pr, const double *x4, const double *g12,
+                        const double *Vbar9, double *xb4, double *gb12, double *V9);
+
 /* ---------------------------------------- scratch-free CFL time step
  * No counterpart in the reference.  For host codes that cannot let a library
  * allocate device memory -- solvers that hand out every device byte from

@@ -27,6 +27,8 @@ EXPORTS = [
     "ns3d_compute_timestep", "ns3d_total_energy", "ns3d_diagnostics", "ns3d_time_advance",
     "ns3d_device_fields", "ns3d_set_stream", "ns3d_synchronize", "ns3d_last_launch_count",
     "ns3d_profile", "ns3d_profile_report", "ns3d_compute_timestep_noalloc",
+    "ns3d_debug_face_vjp", "ns3d_debug_visc_vjp", "ns3d_vjp_rhs", "ns3d_vjp_rk3_step",
+    "ns3d_adjoint_kinetic_energy",
 ]
 
 
@@ -87,6 +89,11 @@ def load() -> C.CDLL:
     lib.ns3d_last_launch_count.argtypes = [h, C.POINTER(C.c_long)]
     lib.ns3d_profile.argtypes = [h, C.c_int]
     lib.ns3d_profile_report.argtypes = [h, C.c_char_p, C.c_long]
+    lib.ns3d_vjp_rhs.argtypes = [h, C.POINTER(dp), C.POINTER(dp)]
+    lib.ns3d_vjp_rk3_step.argtypes = [h, C.c_double, C.POINTER(dp), C.POINTER(dp)]
+    lib.ns3d_adjoint_kinetic_energy.argtypes = [h, C.c_int, C.c_double, C.c_int, dp, C.POINTER(dp), dp]
+    lib.ns3d_debug_face_vjp.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, dp]
+    lib.ns3d_debug_visc_vjp.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp]
     lib.ns3d_compute_timestep_noalloc.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_double,
                                                   C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     _lib = lib

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/ns3d_b200.h"
+#include "adjoint_api.cuh"
 #include "common.cuh"
 #include "schemes.cuh"
 #include "stage.cuh"
@@ -222,6 +223,15 @@ struct ns3d_handle {
     struct Prof { const char *name; std::vector<cudaEvent_t> ev; long launches; double ms; };
     std::vector<Prof> prof;
     int prof_open = -1;
+    // adjoint workspace (allocated on first use): Ub, Acc, Sb, Rb (interior
+    // layout), face-VJP scratch G, viscous scratch X, velocity gradient
+    void *adj_pool = nullptr;
+    size_t adj_bytes = 0;
+    double *ab[4][5] = {};
+    double *adjG[30] = {};
+    double *adjX[16] = {};
+    double *gvel[3] = {};
+    double **adj_tab = nullptr;  // device tables: [5*b + q] for ab[b][q], [20..22] gvel
 };
 
 namespace {
@@ -421,6 +431,171 @@ int check_state(ns3d_handle *h) {
     return NS3D_OK;
 }
 
+
+// ----------------------------------------------------------------- adjoint
+
+__global__ void to_interior_kernel(const double *src, double *dst, Layout L) {
+    // contiguous Field3D array -> interior layout
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.nx) return;
+    dst[((long)k * L.ny + j) * L.nx + i] = src[((long)(k + NG) * L.sy + (j + NG)) * L.sx + (i + NG)];
+}
+
+__global__ void from_interior_kernel(const double *src, double *dst, Layout L) {
+    // interior layout -> contiguous Field3D array (ghost entries zero)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    const bool in = i >= NG && i < NG + L.nx && j >= NG && j < NG + L.ny && k >= NG && k < NG + L.nz;
+    dst[((long)k * L.sy + j) * L.sx + i] = in ? src[((long)(k - NG) * L.ny + (j - NG)) * L.nx + (i - NG)] : 0.0;
+}
+
+bool adjoint_supported(const ns3d_handle *h, std::string &why) {
+    if (h->mixed) { why = "adjoint: plain FP64 path only"; return false; }
+    if (!(h->bc.periodic[0] && h->bc.periodic[1] && h->bc.periodic[2])) {
+        why = "adjoint: periodic boundaries in all directions only"; return false;
+    }
+    if (h->P.char_recon) { why = "adjoint: component-wise interpolation only"; return false; }
+    if (h->P.interpolation != NS3D_WENO5 && h->P.interpolation != NS3D_MDCD_LINEAR) {
+        why = "adjoint: WENO5 or MDCD_LINEAR interpolation only"; return false;
+    }
+    const int rs = h->P.riemann_solver;
+    if (rs != NS3D_ROE && rs != NS3D_RUSANOV && rs != NS3D_HLL) {
+        why = "adjoint: Roe, Rusanov or HLL flux only"; return false;
+    }
+    return true;
+}
+
+int ensure_adjoint(ns3d_handle *h) {
+    if (h->adj_pool) return NS3D_OK;
+    const long n = (long)h->L64.nx * h->L64.ny * h->L64.nz;
+    const long n_al = ((n + 31) / 32) * 32;
+    const size_t arrays = 20 + 30 + 16 + 3;
+    const size_t bytes = arrays * n_al * 8 + 4096;
+    cudaError_t e = cudaMalloc(&h->adj_pool, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); h->adj_pool = nullptr; return fail(h, NS3D_ERR_OOM, "adjoint workspace"); }
+    h->adj_bytes = bytes;
+    double *p = (double *)h->adj_pool;
+    for (int b = 0; b < 4; ++b)
+        for (int q = 0; q < 5; ++q) { h->ab[b][q] = p; p += n_al; }
+    for (int q = 0; q < 30; ++q) { h->adjG[q] = p; p += n_al; }
+    for (int q = 0; q < 16; ++q) { h->adjX[q] = p; p += n_al; }
+    for (int q = 0; q < 3; ++q) { h->gvel[q] = p; p += n_al; }
+    h->adj_tab = (double **)p;
+    void *tab[23];
+    for (int b = 0; b < 4; ++b)
+        for (int q = 0; q < 5; ++q) tab[5 * b + q] = h->ab[b][q];
+    for (int q = 0; q < 3; ++q) tab[20 + q] = h->gvel[q];
+    CK(h, cudaMemcpy(h->adj_tab, tab, sizeof(tab), cudaMemcpyHostToDevice), "adjoint tables");
+    return NS3D_OK;
+}
+
+AdjArgs adj_args(ns3d_handle *h, double *const W[5], const double *const Rb[5], double *const Ub[5]) {
+    AdjArgs a;
+    for (int q = 0; q < 5; ++q) { a.W[q] = W[q]; a.Rb[q] = Rb[q]; a.Ub[q] = Ub[q]; }
+    for (int q = 0; q < 30; ++q) a.G[q] = h->adjG[q];
+    for (int q = 0; q < 16; ++q) a.X[q] = h->adjX[q];
+    a.L = h->L64;
+    a.inv_h[0] = h->ph.inv_dx; a.inv_h[1] = h->ph.inv_dy; a.inv_h[2] = h->ph.inv_dz;
+    a.gamma = h->ph.gamma; a.Rgas = h->ph.Rgas; a.mu0 = h->ph.mu; a.S = h->ph.S; a.cpr = h->ph.Cp / h->ph.Pr;
+    a.interp = h->P.interpolation; a.riemann = h->P.riemann_solver == NS3D_HLL ? 3 : h->P.riemann_solver;
+    for (int m = 0; m < 6; ++m) a.lin[m] = h->sp64.lin[m];
+    a.first = 0;
+    return a;
+}
+
+// Ub_target += (dR/dU at W)^T Rb
+int vjp_rhs_async(ns3d_handle *h, double *const W[5], int rb_slot, int target_slot) {
+    AdjArgs a = adj_args(h, W, h->ab[rb_slot], h->ab[target_slot]);
+    cudaError_t e = adj_rhs_vjp(a, h->stream, &h->launches);
+    if (e != cudaSuccess) return cuda_fail(h, e, "adjoint kernels");
+    return NS3D_OK;
+}
+
+// y = beta*y + alpha*x on adjoint slots
+int axpby_slot(ns3d_handle *h, int y, int x, double alpha, double beta) {
+    const long n = (long)h->L64.nx * h->L64.ny * h->L64.nz;
+    cudaError_t e = adj_axpby(h->adj_tab + 5 * y, h->adj_tab + 5 * x, alpha, beta, n, h->stream);
+    h->launches += 1;
+    if (e != cudaSuccess) return cuda_fail(h, e, "axpby");
+    return NS3D_OK;
+}
+
+// Backward through one RK3 step whose stage states are W0, W1, W2.
+// Slot 0 holds the adjoint of the step's result on entry and of its input on
+// exit; slots 1 (accumulator), 2 (stage adjoint), 3 (rhs adjoint) are scratch.
+//   U1 = U0 + dt R(U0); U2 = 3/4 U0 + 1/4 (U1 + dt R(U1)); U3 = 1/3 U0 + 2/3 (U2 + dt R(U2))
+int vjp_step_async(ns3d_handle *h, double *const W0[5], double *const W1[5], double *const W2[5], double dt) {
+    int r;
+    enum { UB = 0, ACC = 1, SB = 2, RB = 3 };
+    if ((r = axpby_slot(h, RB, UB, (2.0 / 3.0) * dt, 0.0))) return r;
+    if ((r = axpby_slot(h, ACC, UB, 1.0 / 3.0, 0.0))) return r;
+    if ((r = axpby_slot(h, SB, UB, 2.0 / 3.0, 0.0))) return r;
+    if ((r = vjp_rhs_async(h, W2, RB, SB))) return r;          // SB = adjoint of U2
+    if ((r = axpby_slot(h, RB, SB, 0.25 * dt, 0.0))) return r;
+    if ((r = axpby_slot(h, ACC, SB, 0.75, 1.0))) return r;
+    if ((r = axpby_slot(h, SB, SB, 0.0, 0.25))) return r;
+    if ((r = vjp_rhs_async(h, W1, RB, SB))) return r;          // SB = adjoint of U1
+    if ((r = axpby_slot(h, RB, SB, dt, 0.0))) return r;
+    if ((r = axpby_slot(h, ACC, SB, 1.0, 1.0))) return r;
+    if ((r = vjp_rhs_async(h, W0, RB, ACC))) return r;         // ACC = adjoint of U0
+    return axpby_slot(h, UB, ACC, 1.0, 0.0);
+}
+
+// One forward step that also stores its three stage states.
+int rk3_async_store(ns3d_handle *h, double dt, double *const st[3][5]) {
+    const size_t bytes = (size_t)h->L64.plane * 8;
+    const int s0 = h->s0, b1 = (s0 + 1) % 3, b2 = (s0 + 2) % 3;
+    int r;
+    for (int q = 0; q < 5; ++q) CK(h, cudaMemcpyAsync(st[0][q], h->S[s0][q], bytes, cudaMemcpyDeviceToDevice, h->stream), "store");
+    if ((r = compute_rhs_async(h))) return r;
+    if ((r = stage_async(h, 1, s0, s0, b1, dt))) return r;
+    for (int q = 0; q < 5; ++q) CK(h, cudaMemcpyAsync(st[1][q], h->S[b1][q], bytes, cudaMemcpyDeviceToDevice, h->stream), "store");
+    h->s0 = b1;
+    if ((r = compute_rhs_async(h))) { h->s0 = s0; return r; }
+    if ((r = stage_async(h, 2, s0, b1, b2, dt))) { h->s0 = s0; return r; }
+    for (int q = 0; q < 5; ++q) CK(h, cudaMemcpyAsync(st[2][q], h->S[b2][q], bytes, cudaMemcpyDeviceToDevice, h->stream), "store");
+    h->s0 = b2;
+    if ((r = compute_rhs_async(h))) { h->s0 = s0; return r; }
+    if ((r = stage_async(h, 3, s0, b2, b1, dt))) { h->s0 = s0; return r; }
+    h->s0 = b1;
+    return NS3D_OK;
+}
+
+// T of the current state (after the state buffer was overwritten by a copy)
+int refresh_T(ns3d_handle *h) {
+    dim3 g = cell_grid(h->L64, true, 128);
+    temp_kernel64<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), h->T64, h->L64, h->ph.Rgas);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "temperature");
+    return NS3D_OK;
+}
+
+int upload_interior_slot(ns3d_handle *h, const double *const host[5], int slot) {
+    const Layout &L = h->L64;
+    const size_t n = (size_t)L.sx * L.sy * L.sz;
+    const int stg = (h->s0 + 1) % 3;
+    for (int q = 0; q < 5; ++q) {
+        CK(h, cudaMemcpyAsync(h->S[stg][q], host[q], n * 8, cudaMemcpyHostToDevice, h->stream), "upload adjoint");
+        to_interior_kernel<<<cell_grid(L, false, 128), 128, 0, h->stream>>>(h->S[stg][q], h->ab[slot][q], L);
+        h->launches += 1;
+    }
+    CK(h, cudaGetLastError(), "to_interior");
+    return NS3D_OK;
+}
+
+int download_interior_slot(ns3d_handle *h, int slot, double *const host[5]) {
+    const Layout &L = h->L64;
+    const size_t n = (size_t)L.sx * L.sy * L.sz;
+    const int stg = (h->s0 + 1) % 3;
+    for (int q = 0; q < 5; ++q) {
+        from_interior_kernel<<<cell_grid(L, true, 128), 128, 0, h->stream>>>(h->ab[slot][q], h->S[stg][q], L);
+        h->launches += 1;
+        CK(h, cudaMemcpyAsync(host[q], h->S[stg][q], n * 8, cudaMemcpyDeviceToHost, h->stream), "download adjoint");
+    }
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return NS3D_OK;
+}
+
 bool valid_params(const ns3d_params *p, const ns3d_grid *g, std::string &why) {
     if (p->interpolation == NS3D_ZERO) {
         why = "ZERO interpolation sets ghost_layers=1 while the flux difference and viscous stencils read "
@@ -592,6 +767,7 @@ int ns3d_destroy(ns3d_handle *h) {
         for (auto e : p.ev) cudaEventDestroy(e);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     if (h->pool) cudaFree(h->pool);
+    if (h->adj_pool) cudaFree(h->adj_pool);
     delete h;
     return NS3D_OK;
 }
@@ -954,6 +1130,147 @@ int ns3d_device_fields(ns3d_handle *h, int what, void *ptrs[5], long layout[6]) 
         return fail(h, NS3D_ERR_INVALID_ARG, "group not resident on the device in this precision");
     }
     layout[0] = L->sx; layout[1] = L->sy; layout[2] = L->sz; layout[3] = L->px; layout[4] = L->off; layout[5] = esz;
+    return NS3D_OK;
+}
+
+int ns3d_vjp_rhs(ns3d_handle *h, const double *const rbar[5], double *const ubar[5]) {
+    if (!h || !rbar || !ubar) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    std::string why;
+    if (!adjoint_supported(h, why)) return fail(h, NS3D_ERR_CONFIG, why);
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    if ((r = ensure_adjoint(h))) return r;
+    if ((r = upload_interior_slot(h, rbar, 3))) return r;
+    if ((r = axpby_slot(h, 0, 0, 0.0, 0.0))) return r;
+    if ((r = vjp_rhs_async(h, h->S[h->s0], 3, 0))) return r;
+    return download_interior_slot(h, 0, ubar);
+}
+
+int ns3d_vjp_rk3_step(ns3d_handle *h, double dt, const double *const ubar_next[5], double *const ubar[5]) {
+    if (!h || !ubar_next || !ubar) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    std::string why;
+    if (!adjoint_supported(h, why)) return fail(h, NS3D_ERR_CONFIG, why);
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    if ((r = ensure_adjoint(h))) return r;
+    // stage states of the step from the current state; the state is restored
+    const size_t bytes = (size_t)h->L64.plane * 8;
+    double *buf = nullptr;
+    CK(h, cudaMalloc(&buf, 15 * bytes), "stage buffers");
+    double *st[3][5];
+    for (int b = 0; b < 3; ++b)
+        for (int q = 0; q < 5; ++q) st[b][q] = buf + (size_t)(5 * b + q) * h->L64.plane;
+    const int s_keep = h->s0;
+    r = rk3_async_store(h, dt, st);
+    if (!r) {
+        for (int q = 0; q < 5; ++q)
+            cudaMemcpyAsync(h->S[s_keep][q], st[0][q], bytes, cudaMemcpyDeviceToDevice, h->stream);
+        h->s0 = s_keep;
+        r = refresh_T(h);
+        if (!r) r = upload_interior_slot(h, ubar_next, 0);
+    }
+    if (!r) r = vjp_step_async(h, st[0], st[1], st[2], dt);
+    if (!r) r = download_interior_slot(h, 0, ubar);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(buf);
+    return r;
+}
+
+int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int checkpoint_every, double *J,
+                                double *const grad[3], double stats[4]) {
+    if (!h || !J || !grad || nsteps < 1 || checkpoint_every < 1) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    std::string why;
+    if (!adjoint_supported(h, why)) return fail(h, NS3D_ERR_CONFIG, why);
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    if ((r = ensure_adjoint(h))) return r;
+    const int ce = checkpoint_every;
+    const int nck = (nsteps + ce - 1) / ce;
+    const size_t plane = (size_t)h->L64.plane, bytes = plane * 8;
+    // checkpoints (nck states) + one segment of stage states (ce x 3 states)
+    const size_t store_bytes = (size_t)(nck + 3 * ce) * 5 * bytes;
+    double *store = nullptr;
+    CK(h, cudaMalloc(&store, store_bytes), "checkpoint storage");
+    auto ck = [&](int c, int q) { return store + ((size_t)c * 5 + q) * plane; };
+    auto seg = [&](int step, int stage, int q) { return store + ((size_t)(nck + 3 * step + stage) * 5 + q) * plane; };
+    cudaEvent_t e0, e1, em, e2;
+    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&em); cudaEventCreate(&e2);
+    const int s_init = h->s0;
+    double Jv = 0.0;
+    cudaEventRecord(e0, h->stream);
+    // ---- forward with checkpoints every ce steps
+    for (int n = 0; n < nsteps && !r; ++n) {
+        if (n % ce == 0)
+            for (int q = 0; q < 5; ++q)
+                if (cudaMemcpyAsync(ck(n / ce, q), h->S[h->s0][q], bytes, cudaMemcpyDeviceToDevice, h->stream))
+                    r = fail(h, NS3D_ERR_CUDA, "checkpoint copy");
+        if (!r) r = rk3_async(h, dt);
+    }
+    cudaEventRecord(e1, h->stream);
+    long recomputed = 0;
+    if (!r) {
+        // objective of the final state and its adjoint seed
+        AdjArgs a = adj_args(h, h->S[h->s0], h->ab[3], h->ab[0]);
+        cudaError_t e = adj_ke_seed(a, h->ph.dx * h->ph.dy * h->ph.dz, h->adj_tab, h->stream);
+        if (e != cudaSuccess) r = cuda_fail(h, e, "seed");
+    }
+    if (!r) {
+        double d[6];
+        r = ns3d_diagnostics(h, d);
+        Jv = d[0];
+    }
+    cudaEventRecord(em, h->stream);  // backward pass starts here
+    // ---- backward: per segment recompute the stage states, then step back
+    for (int c = nck - 1; c >= 0 && !r; --c) {
+        const int n0 = c * ce, n1 = (n0 + ce < nsteps) ? n0 + ce : nsteps;
+        for (int q = 0; q < 5; ++q)
+            cudaMemcpyAsync(h->S[h->s0][q], ck(c, q), bytes, cudaMemcpyDeviceToDevice, h->stream);
+        r = refresh_T(h);
+        for (int n = n0; n < n1 && !r; ++n) {
+            double *st[3][5];
+            for (int b = 0; b < 3; ++b)
+                for (int q = 0; q < 5; ++q) st[b][q] = seg(n - n0, b, q);
+            r = rk3_async_store(h, dt, st);
+            ++recomputed;
+        }
+        for (int n = n1 - 1; n >= n0 && !r; --n) {
+            double *W0[5], *W1[5], *W2[5];
+            for (int q = 0; q < 5; ++q) { W0[q] = seg(n - n0, 0, q); W1[q] = seg(n - n0, 1, q); W2[q] = seg(n - n0, 2, q); }
+            r = vjp_step_async(h, W0, W1, W2, dt);
+        }
+    }
+    cudaEventRecord(e2, h->stream);
+    if (!r) {
+        // initial state back into the handle, gradient w.r.t. the initial velocity
+        for (int q = 0; q < 5; ++q)
+            cudaMemcpyAsync(h->S[s_init][q], ck(0, q), bytes, cudaMemcpyDeviceToDevice, h->stream);
+        h->s0 = s_init;
+        AdjArgs a = adj_args(h, h->S[h->s0], h->ab[3], h->ab[0]);
+        cudaError_t e = adj_velocity_grad(a, h->adj_tab, h->adj_tab + 20, h->stream);
+        if (e != cudaSuccess) r = cuda_fail(h, e, "velocity gradient");
+        const size_t nb = (size_t)h->L64.nx * h->L64.ny * h->L64.nz * 8;
+        for (int q = 0; q < 3 && !r; ++q)
+            if (cudaMemcpyAsync(grad[q], h->gvel[q], nb, cudaMemcpyDeviceToHost, h->stream))
+                r = fail(h, NS3D_ERR_CUDA, "gradient copy");
+        // T of the restored state for the next RHS
+        if (!r) r = refresh_T(h);
+    }
+    cudaStreamSynchronize(h->stream);
+    float fwd_ms = 0.f, adj_ms = 0.f;
+    cudaEventElapsedTime(&fwd_ms, e0, e1);
+    cudaEventElapsedTime(&adj_ms, em, e2);
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(em); cudaEventDestroy(e2);
+    cudaFree(store);
+    if (r) return r;
+    *J = Jv;
+    if (stats) {
+        stats[0] = fwd_ms; stats[1] = adj_ms;
+        stats[2] = (double)(store_bytes + h->adj_bytes);
+        stats[3] = (double)recomputed;
+    }
     return NS3D_OK;
 }
 

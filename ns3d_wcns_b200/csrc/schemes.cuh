@@ -11,6 +11,10 @@
 
 #include "common.cuh"
 
+#ifndef NS3D_HD
+#define NS3D_HD __host__ __device__ __forceinline__
+#endif
+
 namespace ns3d {
 
 enum { I_WENO5 = 0, I_ZERO = 1, I_MDCD_LINEAR = 2, I_MDCD_HYBRID = 3 };
@@ -31,7 +35,7 @@ struct SchemeParams {
 // the 5 left-biased points f0..f4, weights 1/16, 5/8, 5/16, eps = 1e-6.
 // The three divisions of the normalised weights are folded into one.
 template <typename R>
-__device__ __forceinline__ R weno5(R f0, R f1, R f2, R f3, R f4) {
+NS3D_HD R weno5(R f0, R f1, R f2, R f3, R f4) {
     const R eps = R(1e-6);
     const R c13 = R(13.0 / 12.0);
     R t, u;
@@ -54,7 +58,7 @@ __device__ __forceinline__ R weno5(R f0, R f1, R f2, R f3, R f4) {
 
 // mdcd_linear_interpolate, interpolation.cpp:118-133.
 template <typename R>
-__device__ __forceinline__ R mdcd_linear(const R *c, R f0, R f1, R f2, R f3, R f4, R f5) {
+NS3D_HD R mdcd_linear(const R *c, R f0, R f1, R f2, R f3, R f4, R f5) {
     return c[0] * f0 + c[1] * f1 + c[2] * f2 + c[3] * f3 + c[4] * f4 + c[5] * f5;
 }
 
@@ -63,7 +67,7 @@ __device__ __forceinline__ R mdcd_linear(const R *c, R f0, R f1, R f2, R f3, R f
 // sums are (20,0,0,0,0,0), so beta3(f) = Q(f - f0) + f0^2/6048 exactly; the
 // FP32 path evaluates that split form, which avoids the cancellation of the
 // expanded form (terms ~1e3 f^2 summing to ~1e-4 f^2).
-__device__ __forceinline__ double mdcd_beta3(double f0, double f1, double f2, double f3, double f4,
+NS3D_HD double mdcd_beta3(double f0, double f1, double f2, double f3, double f4,
                                              double f5) {
     return (271799.0 * (f0 * f0) +
             f0 * (-2380800.0 * f1 + 4086352.0 * f2 - 3462252.0 * f3 + 1458762.0 * f4 - 245620.0 * f5) +
@@ -72,7 +76,7 @@ __device__ __forceinline__ double mdcd_beta3(double f0, double f1, double f2, do
             f3 * (17195652.0 * f3 - 15880404.0 * f4 + 2863984.0 * f5) +
             f4 * (3824847.0 * f4 - 1429976.0 * f5) + 139633.0 * (f5 * f5)) / 120960.0;
 }
-__device__ __forceinline__ float mdcd_beta3(float f0, float f1, float f2, float f3, float f4, float f5) {
+NS3D_HD float mdcd_beta3(float f0, float f1, float f2, float f3, float f4, float f5) {
     const float d1 = f1 - f0, d2 = f2 - f0, d3 = f3 - f0, d4 = f4 - f0, d5 = f5 - f0;
     float q = d1 * (5653317.f * d1 - 20427884.f * d2 + 17905032.f * d3 - 7727988.f * d4 + 1325006.f * d5) +
               d2 * (19510972.f * d2 - 35817664.f * d3 + 15929912.f * d4 - 2792660.f * d5) +
@@ -85,7 +89,7 @@ __device__ __forceinline__ float mdcd_beta3(float f0, float f1, float f2, float 
 // min(sai1, sai2) > 0.4 is evaluated as two cross-multiplied comparisons
 // (denominators are positive).
 template <typename R>
-__device__ __forceinline__ R mdcd_hybrid(const R *lin, const R *hd, R f0, R f1, R f2, R f3, R f4, R f5) {
+NS3D_HD R mdcd_hybrid(const R *lin, const R *hd, R f0, R f1, R f2, R f3, R f4, R f5) {
     const R eps = R(0.9 * 0.4 / (1.0 - 0.9 * 0.4) * 1e-4);
     R a1 = fabs(f2 - f1) + fabs(f2 - R(2) * f1 + f0);
     R b1 = fabs(f2 - f3) + fabs(f2 - R(2) * f3 + f4);
@@ -120,7 +124,7 @@ __device__ __forceinline__ R mdcd_hybrid(const R *lin, const R *hd, R f0, R f1, 
 // interpolate_select, interpolation.cpp:13-77, for the left state (flag +1,
 // stencil f[0..5]) or the right state (flag -1, reversed stencil).
 template <typename R, int INTERP>
-__device__ __forceinline__ R interp_side(const SchemeParams<R> &sp, const R *f, bool right) {
+NS3D_HD R interp_side(const SchemeParams<R> &sp, const R *f, bool right) {
     const int it = INTERP == RUNTIME ? sp.interp : INTERP;
     R g0, g1, g2, g3, g4, g5;
     if (!right) { g0 = f[0]; g1 = f[1]; g2 = f[2]; g3 = f[3]; g4 = f[4]; g5 = f[5]; }
@@ -135,14 +139,14 @@ __device__ __forceinline__ R interp_side(const SchemeParams<R> &sp, const R *f, 
 template <int DIR, typename R>
 struct Side {
     R r, ir, u, v, w, E, p, un;
-    __device__ __forceinline__ void load(const R *U, R g) {
+    NS3D_HD void load(const R *U, R g) {
         r = U[0]; ir = R(1) / r;
         u = U[1] * ir; v = U[2] * ir; w = U[3] * ir; E = U[4];
         p = (E - R(0.5) * r * (u * u + v * v + w * w)) * (g - R(1));
         un = DIR == 0 ? u : (DIR == 1 ? v : w);
     }
     // physical flux of the state along the face normal (InviscousFlux.cpp:333-346)
-    __device__ __forceinline__ void flux(R *F) const {
+    NS3D_HD void flux(R *F) const {
         R m = r * un;
         F[0] = m;
         F[1] = m * u + (DIR == 0 ? p : R(0));
@@ -158,7 +162,7 @@ struct Side {
 // the two acoustic projections are formed.  Harten entropy fix with
 // delta = 0.1 max|lambda| = 0.1 (|V| + c) as the reference.
 template <int DIR, typename R>
-__device__ __forceinline__ void roe_flux(const R *UL, const R *UR, R g, R *F) {
+NS3D_HD void roe_flux(const R *UL, const R *UR, R g, R *F) {
     Side<DIR, R> L, Rt;
     L.load(UL, g); Rt.load(UR, g);
     R FL[5], FR[5];
@@ -209,7 +213,7 @@ __device__ __forceinline__ void roe_flux(const R *UL, const R *UR, R g, R *F) {
 
 // Rusanov_Riemann_solver, InviscousFlux.cpp:270-311.
 template <int DIR, typename R>
-__device__ __forceinline__ void rusanov_flux(const R *UL, const R *UR, R g, R *F) {
+NS3D_HD void rusanov_flux(const R *UL, const R *UR, R g, R *F) {
     Side<DIR, R> L, Rt;
     L.load(UL, g); Rt.load(UR, g);
     R FL[5], FR[5];
@@ -222,7 +226,7 @@ __device__ __forceinline__ void rusanov_flux(const R *UL, const R *UR, R g, R *F
 
 // HLL_Riemann_solver, InviscousFlux.cpp:384-447 (Davis wave speeds).
 template <int DIR, typename R>
-__device__ __forceinline__ void hll_flux(const R *UL, const R *UR, R g, R *F) {
+NS3D_HD void hll_flux(const R *UL, const R *UR, R g, R *F) {
     Side<DIR, R> L, Rt;
     L.load(UL, g); Rt.load(UR, g);
     R FL[5], FR[5];
@@ -245,7 +249,7 @@ __device__ __forceinline__ void hll_flux(const R *UL, const R *UR, R g, R *F) {
 
 // HLLC star-region flux, InviscousFlux.cpp:537-591 (and :663-715 for HLLC_p).
 template <int DIR, typename R>
-__device__ __forceinline__ void hllc_star(const Side<DIR, R> &S, const R *U, const R *Fs, R Sk, R SM,
+NS3D_HD void hllc_star(const Side<DIR, R> &S, const R *U, const R *Fs, R Sk, R SM,
                                           R *F) {
     R dk = Sk - S.un;
     R rs = S.r * dk / (Sk - SM);
@@ -261,7 +265,7 @@ __device__ __forceinline__ void hllc_star(const Side<DIR, R> &S, const R *U, con
 // HLLC_Riemann_solver, InviscousFlux.cpp:449-592: Davis S_L/S_R, Batten S_M
 // (Roe-averaged normal velocity when the S_M denominator is below 1e-12).
 template <int DIR, typename R>
-__device__ __forceinline__ void hllc_flux(const R *UL, const R *UR, R g, R *F) {
+NS3D_HD void hllc_flux(const R *UL, const R *UR, R g, R *F) {
     Side<DIR, R> L, Rt;
     L.load(UL, g); Rt.load(UR, g);
     R aL = sqrt(g * L.p * L.ir), aR = sqrt(g * Rt.p * Rt.ir);
@@ -285,7 +289,7 @@ __device__ __forceinline__ void hllc_flux(const R *UL, const R *UR, R g, R *F) {
 
 // HLLC_p_Riemann_solver, InviscousFlux.cpp:594-717: PVRS p*, Toro speeds.
 template <int DIR, typename R>
-__device__ __forceinline__ void hllc_p_flux(const R *UL, const R *UR, R g, R *F) {
+NS3D_HD void hllc_p_flux(const R *UL, const R *UR, R g, R *F) {
     Side<DIR, R> L, Rt;
     L.load(UL, g); Rt.load(UR, g);
     R aL = sqrt(g * L.p * L.ir), aR = sqrt(g * Rt.p * Rt.ir);
@@ -307,7 +311,7 @@ __device__ __forceinline__ void hllc_p_flux(const R *UL, const R *UR, R g, R *F)
 // Ku = 0.75, pressure clamped at 1e-12; the pressure diffusion uses the
 // x-velocity difference u_R - u_L in every direction, as the reference).
 template <int DIR, typename R>
-__device__ __forceinline__ void ausm_flux(const R *UL, const R *UR, R g, R *F) {
+NS3D_HD void ausm_flux(const R *UL, const R *UR, R g, R *F) {
     const R Kp = R(0.25), Ku = R(0.75);
     Side<DIR, R> L, Rt;
     L.load(UL, g); Rt.load(UR, g);
@@ -339,7 +343,7 @@ __device__ __forceinline__ void ausm_flux(const R *UL, const R *UR, R g, R *F) {
 }
 
 template <int DIR, typename R, int RS>
-__device__ __forceinline__ void riemann(const SchemeParams<R> &sp, const R *UL, const R *UR, R *F) {
+NS3D_HD void riemann(const SchemeParams<R> &sp, const R *UL, const R *UR, R *F) {
     const int rs = RS == RUNTIME ? sp.riemann : RS;
     const R g = sp.gamma;
     if (RS == R_ROE || (RS == RUNTIME && rs == R_ROE)) roe_flux<DIR, R>(UL, UR, g, F);
@@ -356,7 +360,7 @@ __device__ __forceinline__ void riemann(const SchemeParams<R> &sp, const R *UL, 
 // WCNS_Riemann_InviscidFlux does for characteristic interpolation
 // (InviscousFlux.cpp:166-231 with :849-987).  w = primitive (rho,u,v,w,p).
 template <int DIR, typename R>
-__device__ __forceinline__ void cell_eigen(const R *w, R g, R Lm[5][5], R Rm[5][5]) {
+NS3D_HD void cell_eigen(const R *w, R g, R Lm[5][5], R Rm[5][5]) {
     const R nx = DIR == 0 ? R(1) : R(0), ny = DIR == 1 ? R(1) : R(0), nz = DIR == 2 ? R(1) : R(0);
     const R gm1 = g - R(1);
     R r = w[0], u = w[1], v = w[2], ww = w[3], p = w[4];
@@ -403,7 +407,7 @@ __device__ __forceinline__ void cell_eigen(const R *w, R g, R Lm[5][5], R Rm[5][
 // U[n][m]: conserved stencil of cells i-2..i+3; wi / wi1: primitives of the
 // cells i and i+1 (characteristic bases of the left / right states).
 template <int DIR, typename R, int INTERP, int RS, int CHAR>
-__device__ __forceinline__ void wcns_face(const SchemeParams<R> &sp, const R U[5][6], const R *wi,
+NS3D_HD void wcns_face(const SchemeParams<R> &sp, const R U[5][6], const R *wi,
                                           const R *wi1, R *F) {
     R UL[5], UR[5];
     const bool ch = CHAR == RUNTIME ? (sp.char_recon != 0) : (CHAR != 0);

@@ -156,6 +156,32 @@ class Solver:
         self.lib.ns3d_last_launch_count(self.h, C.byref(x))
         return x.value
 
+    # -- adjoint
+    def vjp_rhs(self, rbar: np.ndarray) -> np.ndarray:
+        """(dR/dU)^T rbar at the current state; rbar (5, sz, sy, sx)."""
+        rb = [np.ascontiguousarray(rbar[q], dtype=np.float64) for q in range(5)]
+        out = np.zeros((5,) + self.shape)
+        self._check(self.lib.ns3d_vjp_rhs(self.h, self._ptrs(rb), self._ptrs([out[q] for q in range(5)])))
+        return out
+
+    def vjp_rk3_step(self, dt: float, ubar_next: np.ndarray) -> np.ndarray:
+        ub = [np.ascontiguousarray(ubar_next[q], dtype=np.float64) for q in range(5)]
+        out = np.zeros((5,) + self.shape)
+        self._check(self.lib.ns3d_vjp_rk3_step(self.h, C.c_double(dt), self._ptrs(ub),
+                                               self._ptrs([out[q] for q in range(5)])))
+        return out
+
+    def adjoint_kinetic_energy(self, nsteps: int, dt: float, checkpoint_every: int = 20):
+        """(J, grad (3, nz, ny, nx), stats dict) -- see ns3d_adjoint_kinetic_energy."""
+        n = (self.G.global_nz, self.G.global_ny, self.G.global_nx)
+        grad = np.zeros((3,) + n)
+        J = C.c_double()
+        st = (C.c_double * 4)()
+        self._check(self.lib.ns3d_adjoint_kinetic_energy(self.h, int(nsteps), C.c_double(dt), int(checkpoint_every),
+                                                         C.byref(J), self._ptrs([grad[q] for q in range(3)]), st))
+        return J.value, grad, {"forward_ms": st[0], "adjoint_ms": st[1], "adjoint_bytes": st[2],
+                               "recomputed_steps": st[3]}
+
     def profile(self, enable: bool = True) -> None:
         self._check(self.lib.ns3d_profile(self.h, int(enable)))
 
