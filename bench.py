@@ -166,6 +166,49 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------- adjoint
+
+def adjoint_report(device: int, n: int = 64, nsteps: int = 200, dt: float = 2e-3, ce: int = 20, ndir: int = 16):
+    """Config 4: 64^3 isotropic, Re 200, dt 2e-3, 200 RK3 steps, checkpoint every 20;
+    gradient of the final kinetic energy w.r.t. the initial velocity, checked
+    against central finite differences (h = 1e-6) on ndir seeded directions."""
+    import numpy as np
+    import math
+    from ns3d_wcns_b200.config import make_params
+    from ns3d_wcns_b200.initial import isotropic_state
+    from ns3d_wcns_b200.solver import Solver
+    P, G = make_params(n=(n, n, n), L=(2 * math.pi,) * 3, Ma=0.3, Re=200.0, Pr=0.72, dt_fixed=dt,
+                       interpolation=0, riemann=0, S_ref=110.4 / 273.15)
+    st = isotropic_state((n, n, n), P.gamma, P.Ma, seed=4)
+    rng = np.random.default_rng(16)
+    with Solver(P, G, device=device) as s:
+        s.set_interior_primitives(*st)
+        s.rk3_steps(3, dt)  # warm-up
+        s.set_interior_primitives(*st)
+        J, grad, stats = s.adjoint_kinetic_energy(nsteps, dt, ce)
+        s.set_interior_primitives(*st)
+        J2, grad2, stats2 = s.adjoint_kinetic_energy(nsteps, dt, ce)  # warm timing
+        errs = []
+        h = 1e-6
+        for _ in range(ndir):
+            d = rng.standard_normal((3, n, n, n))
+            d /= np.sqrt(np.mean(d * d))
+            Jpm = []
+            for sgn in (1, -1):
+                rho, u, v, w, p = st
+                s.set_interior_primitives(rho, u + sgn * h * d[0], v + sgn * h * d[1], w + sgn * h * d[2], p)
+                s.rk3_steps(nsteps, dt)
+                Jpm.append(s.total_energy())
+            fd = (Jpm[0] - Jpm[1]) / (2 * h)
+            ad = float(np.sum(grad2 * d))
+            errs.append(abs(fd - ad) / abs(fd))
+    return {"config": f"{n}^3 isotropic WENO5+Roe, Re 200, dt {dt}, {nsteps} steps, checkpoint every {ce}",
+            "J": J2, "forward_ms": stats2["forward_ms"], "adjoint_ms": stats2["adjoint_ms"],
+            "adjoint_over_forward": stats2["adjoint_ms"] / stats2["forward_ms"],
+            "peak_adjoint_bytes": stats2["adjoint_bytes"], "fd_directions": ndir, "fd_h": 1e-6,
+            "fd_max_rel_err": max(errs), "fd_median_rel_err": float(np.median(errs))}
+
+
 # --------------------------------------------------------------- GPU arm
 
 def main():
@@ -178,6 +221,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NS3D_BENCH_ALLOW_SHORT"), \
         "at least 3 warm-up steps"
@@ -313,6 +357,10 @@ def main():
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 8,
                "path": "ns3d_upload_primitives + ns3d_compute_timestep + ns3d_rk3_step + ns3d_download"}
 
+    adjoint = None
+    if not args.no_adjoint and rank == 0:
+        adjoint = adjoint_report(local)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
@@ -327,6 +375,7 @@ def main():
             "kernels_ms": {k: round(v["ms"] / max(v["launches"], 1), 4) for k, v in prof.items()},
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "kinetic_energy_end": ke64,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

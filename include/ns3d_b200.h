@@ -203,6 +203,31 @@ int ns3d_vjp_rk3_step(ns3d_handle *h, double dt, const double *const ubar_next[5
 int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int checkpoint_every, double *J,
                                 double *const grad[3], double stats[4]);
 
+/* ------------------------------------------------------------- batched
+ * Many independent small problems of uneven size (e.g. quasi-1D shock tubes,
+ * Nx x 4 x 4) in one persistent launch: each is a full time_advance run
+ * (maincycle.cpp:18-56) of its own grid to its own end time with its own CFL
+ * time step.  No counterpart in the reference (one problem per process).
+ * Plain FP64, inviscid (Re = inf), y and z periodic, any x boundary types,
+ * component-wise interpolation.  Thread-block clusters take problems from an
+ * atomic work queue, largest first; ns3d_batch_autotune times the cluster
+ * size (1,2,4,8) x CTA width (128,256) choices and keeps the fastest. */
+typedef struct ns3d_batch ns3d_batch;
+int ns3d_batch_create(const ns3d_params *params, int n_problems, const ns3d_grid *grids, const double *t_end,
+                      ns3d_batch **out);
+int ns3d_batch_destroy(ns3d_batch *b);
+const char *ns3d_batch_last_error(const ns3d_batch *b);
+/* interior primitives of problem i (nx*ny*nz each) + its ghost fill */
+int ns3d_batch_set_interior_primitives(ns3d_batch *b, int problem, const double *const fields[5]);
+/* one persistent launch (captured in a CUDA graph) to every problem's t_end */
+int ns3d_batch_run(ns3d_batch *b, int max_steps);
+int ns3d_batch_autotune(ns3d_batch *b, int trial_steps, int config_out[2]);
+int ns3d_batch_set_config(ns3d_batch *b, int cluster, int threads);
+/* final time, steps taken, status (0 reached t_end, 1 dt <= 1e-12, 2 max_steps) */
+int ns3d_batch_query(ns3d_batch *b, int problem, double *time, int *steps, int *status);
+/* primitive Field3D arrays (rho,u,v,w,p; sx*sy*sz each) of problem i */
+int ns3d_batch_download(ns3d_batch *b, int problem, double *const out[5]);
+
 /* ------------------------------------------------- verification helpers
  * Host evaluation (no device needed) of the code the adjoint kernels run,
  * for finite-difference checks.  No counterpart in the reference.

@@ -1,0 +1,97 @@
+"""Batched persistent launch (ns3d_batch_*): every problem against the oracle
+running the reference's own dt schedule (maincycle.cpp:18-56) on that
+problem; results independent of the autotuned launch configuration."""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import rel_linf
+from ns3d_wcns_b200.batch import Batch
+from ns3d_wcns_b200.config import GridDesc, make_params
+from ns3d_wcns_b200.initial import shock_tube_state
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_run(P, g, st, t_end, max_steps=100000):
+    from ns3d_wcns_b200.config import make_params as mp
+    Pg, G = mp(n=(g.global_nx, g.global_ny, g.global_nz), L=(1.0, 1.0, 1.0), gamma=P.gamma, Ma=P.Ma, Re=P.Re,
+               cfl=P.cfl, dt_fixed=-1.0, interpolation=int(P.interpolation), riemann=int(P.riemann_solver),
+               bcs=P.bcs)
+    o = oracle.PortSolver(Pg, G)
+    o.set_interior_prims(*st)
+    t, steps = 0.0, 0
+    for _ in range(max_steps):
+        if abs(t_end - t) <= 1e-12:
+            break
+        dt = o.timestep()
+        if t + dt > t_end:
+            dt = t_end - t
+        if dt <= 1e-12:
+            break
+        t += dt
+        o.rk3_step(dt)
+        steps += 1
+        if t >= t_end:
+            break
+    W = np.stack([o.get(k) for k in ("rho", "u", "v", "w", "p")])
+    return W, t, steps
+
+
+def problems(interp=0, rs=0):
+    P, _ = make_params(n=(8, 4, 4), Ma=1.0, Re=math.inf, cfl=0.5, dt_fixed=-1.0, interpolation=interp, riemann=rs,
+                       bcs=(3, 3, 0, 0, 0, 0))
+    rng = np.random.default_rng(2)
+    sizes = [48, 24, 40, 32, 56, 20]
+    grids = [GridDesc(global_nx=s, global_ny=4, global_nz=4, Lx=1.0, Ly=1.0, Lz=1.0) for s in sizes]
+    states, t_end = [], []
+    for s in sizes:
+        left = (rng.uniform(0.1, 1.0), rng.uniform(-1, 1), rng.uniform(0.1, 3.5))
+        right = (rng.uniform(0.1, 1.0), rng.uniform(-1, 1), rng.uniform(0.1, 3.5))
+        states.append(shock_tube_state(s, 4, 4, left, right))
+        t_end.append(rng.uniform(0.03, 0.05))
+    return P, grids, states, t_end
+
+
+@pytest.mark.parametrize("scheme", [(0, 0), (3, 2)])
+def test_batch_matches_oracle_per_problem(gpu_lib, scheme):
+    P, grids, states, t_end = problems(*scheme)
+    with Batch(P, grids, t_end) as b:
+        for i, st in enumerate(states):
+            b.set_interior_primitives(i, *st)
+        b.run()
+        for i, (g, st) in enumerate(zip(grids, states)):
+            W, t, steps = oracle_run(P, g, st, t_end[i])
+            tg, sg, status = b.query(i)
+            assert status == 0 and sg == steps and abs(tg - t) <= 1e-14
+            Wg = b.primitives(i)
+            assert max(rel_linf(a, r) for a, r in zip(Wg, W)) <= 1e-10
+
+
+def test_batch_results_do_not_depend_on_launch_config(gpu_lib):
+    P, grids, states, t_end = problems()
+    outs = []
+    for cfg in [(1, 128), (4, 256), (8, 128)]:
+        with Batch(P, grids, t_end) as b:
+            for i, st in enumerate(states):
+                b.set_interior_primitives(i, *st)
+            b.set_config(*cfg)
+            b.run()
+            outs.append([b.primitives(i) for i in range(len(grids))])
+    for o in outs[1:]:
+        for a, r in zip(o, outs[0]):
+            assert np.array_equal(a, r)
+
+
+def test_autotune_picks_a_valid_config_and_keeps_the_state(gpu_lib):
+    P, grids, states, t_end = problems()
+    with Batch(P, grids, t_end) as b:
+        for i, st in enumerate(states):
+            b.set_interior_primitives(i, *st)
+        cl, th = b.autotune(trial_steps=5)
+        assert cl in (1, 2, 4, 8) and th in (128, 256)
+        b.run()
+        W, t, steps = oracle_run(P, grids[0], states[0], t_end[0])
+        assert max(rel_linf(a, r) for a, r in zip(b.primitives(0), W)) <= 1e-10
