@@ -209,6 +209,74 @@ def adjoint_report(device: int, n: int = 64, nsteps: int = 200, dt: float = 2e-3
             "fd_max_rel_err": max(errs), "fd_median_rel_err": float(np.median(errs))}
 
 
+# --------------------------------------------------------------- batched
+
+def _ref_tube(args):
+    """CPU reference run of one shock tube (spawned process)."""
+    nx, left, right, t_end = args
+    sys.path.insert(0, ROOT)
+    import math
+    from ns3d_wcns_b200.config import make_params
+    from ns3d_wcns_b200.initial import shock_tube_state
+    from oracle import oracle
+    P, G = make_params(n=(nx, 4, 4), L=(1.0, 1.0, 1.0), Ma=1.0, Re=math.inf, cfl=0.5, dt_fixed=-1.0,
+                       interpolation=0, riemann=0, bcs=(3, 3, 0, 0, 0, 0))
+    s = oracle.RefSolver(P, G) if oracle.ref_available() else oracle.PortSolver(P, G)
+    s.set_interior_prims(*shock_tube_state(nx, 4, 4, left, right))
+    t = 0.0
+    while abs(t_end - t) > 1e-12:
+        dt = s.timestep()
+        if t + dt > t_end:
+            dt = t_end - t
+        if dt <= 1e-12:
+            break
+        t += dt
+        s.rk3_step(dt)
+        if t >= t_end:
+            break
+    import numpy as np
+    return np.stack([s.get(k) for k in ("rho", "u", "v", "w", "p")])
+
+
+def batched_report(device: int, n: int = 512, n_ref: int = 2):
+    """Config 5: n quasi-1D shock tubes Nx x 4 x 4, Nx in {200,400,800,1600}, seeded left/right
+    states, t_end in [0.14, 0.2], inviscid WENO5+Roe, CFL 0.5, x Outflow, y/z Periodic; one
+    persistent launch (autotuned clusters, CUDA graph).  L1 error against the reference CPU
+    solver on the first n_ref problems with Nx = 200."""
+    import math
+    import multiprocessing as mp
+    import numpy as np
+    from ns3d_wcns_b200.batch import Batch, shock_tube_problems
+    from ns3d_wcns_b200.config import make_params
+    from ns3d_wcns_b200.initial import shock_tube_state
+    P, _ = make_params(n=(8, 4, 4), Ma=1.0, Re=math.inf, cfl=0.5, dt_fixed=-1.0, interpolation=0, riemann=0,
+                       bcs=(3, 3, 0, 0, 0, 0))
+    grids, left, right, t_end = shock_tube_problems(n, seed=5)
+    with Batch(P, grids, t_end, device=device) as b:
+        for i, g in enumerate(grids):
+            b.set_interior_primitives(i, *shock_tube_state(g.global_nx, 4, 4, left[i], right[i]))
+        cfg = b.autotune(trial_steps=30)
+        for i, g in enumerate(grids):  # fresh start after tuning
+            b.set_interior_primitives(i, *shock_tube_state(g.global_nx, 4, 4, left[i], right[i]))
+        t0 = time.perf_counter()
+        b.run()
+        wall = time.perf_counter() - t0
+        steps = [b.query(i)[1] for i in range(n)]
+        cell_updates = sum(g.global_nx * 16 * s for g, s in zip(grids, steps))
+        sample = [i for i, g in enumerate(grids) if g.global_nx == 200][:n_ref]
+        with mp.get_context("spawn").Pool(len(sample)) as pool:
+            refs = pool.map(_ref_tube, [(200, tuple(left[i]), tuple(right[i]), float(t_end[i])) for i in sample])
+        l1 = []
+        for i, Wr in zip(sample, refs):
+            Wg = b.primitives(i)
+            sl = (slice(None), slice(3, -3), slice(3, -3), slice(3, -3))
+            l1.append(float(np.abs(Wg[sl] - Wr[sl]).sum() / np.abs(Wr[sl]).sum()))
+    return {"config": f"{n} shock tubes Nx x 4 x 4, Nx in {{200,400,800,1600}}, WENO5+Roe, CFL 0.5, t_end 0.14-0.2",
+            "problems_per_s": n / wall, "wall_s": wall, "cell_updates_per_s": cell_updates / wall,
+            "autotuned": {"cluster": cfg[0], "threads": cfg[1]}, "steps_max": max(steps),
+            "ref_l1_rel_err": l1, "ref_sample": f"{len(sample)} problems with Nx=200 vs the reference CPU solver"}
+
+
 # --------------------------------------------------------------- GPU arm
 
 def main():
@@ -222,6 +290,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-problems", type=int, default=512)
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NS3D_BENCH_ALLOW_SHORT"), \
         "at least 3 warm-up steps"
@@ -360,6 +430,9 @@ def main():
     adjoint = None
     if not args.no_adjoint and rank == 0:
         adjoint = adjoint_report(local)
+    batched = None
+    if not args.no_batch and rank == 0:
+        batched = batched_report(local, args.batch_problems)
 
     if rank == 0:
         line = {
@@ -376,6 +449,7 @@ def main():
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "kinetic_energy_end": ke64,
             "adjoint": adjoint,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
