@@ -277,6 +277,145 @@ def batched_report(device: int, n: int = 512, n_ref: int = 2):
             "ref_l1_rel_err": l1, "ref_sample": f"{len(sample)} problems with Nx=200 vs the reference CPU solver"}
 
 
+# --------------------------------------------------------------- accuracy
+
+def _interior(a):
+    return a[..., 3:-3, 3:-3, 3:-3]
+
+
+def _advance_logged(step_fn, t, t_out, ke_fn, log):
+    """time_advance's dt schedule one step at a time (maincycle.cpp:18-56), logging (t, KE)."""
+    while abs(t_out - t) > 1e-12:
+        t_new = step_fn(t, t_out)
+        if t_new == t:
+            break
+        t = t_new
+        log.append((t, ke_fn()))
+    return t
+
+
+def _ref_series(args):
+    """Reference CPU run (oracle/_ref) of the isotropic workload to t_outs (spawned process)."""
+    n, t_outs, interp, riemann = args
+    sys.path.insert(0, ROOT)
+    import math
+    from ns3d_wcns_b200 import analysis
+    from ns3d_wcns_b200.config import make_params
+    from ns3d_wcns_b200.initial import isotropic_state
+    from oracle import oracle
+    P, G = make_params(n=(n, n, n), L=(2 * math.pi,) * 3, Ma=0.3, Re=400.0, Pr=0.72, cfl=0.5, dt_fixed=-1.0,
+                       interpolation=interp, riemann=riemann, S_ref=110.4 / 273.15)
+    s = oracle.RefSolver(P, G) if oracle.ref_available() else oracle.PortSolver(P, G)
+    s.set_interior_prims(*isotropic_state((n, n, n), 1.4, 0.3, seed=0))
+
+    def step(t, t_out):
+        dt = s.timestep()
+        if t + dt > t_out:
+            dt = t_out - t
+        if dt <= 1e-12:
+            return t
+        s.rk3_step(dt)
+        return t + dt
+
+    log, stats, t = [], {}, 0.0
+    dV = (2 * math.pi / n) ** 3
+    for t_out in t_outs:
+        t = _advance_logged(step, t, t_out, s.total_energy, log)
+        f = {k: _interior(s.get(k)) for k in ("rho", "u", "v", "w", "T")}
+        st = analysis.turbulence_stats(f["rho"], f["u"], f["v"], f["w"], f["T"], 1.0 / 400.0, 110.4 / 273.15, dV)
+        stats[t_out] = {"total_energy": st["total_energy"], "dissipation": st["dissipation"]}
+    return {"log": log, "stats": stats, "kind": "reference" if oracle.ref_available() else "port"}
+
+
+def accuracy_report(device: int, sizes=(256,), t_outs=(0.5, 1.0), ref_n: int = 0, series_dt: float = 0.1):
+    """Mixed FP32/FP64 path against the plain FP64 path (itself pinned to the oracle at <= 1e-10
+    over 10 steps) on the isotropic workload: relative L2 error of rho, u, v, w, E and of the
+    spectrum E(k), k = 1..N/3, relative error of the kinetic energy and of the dissipation
+    2 nu sum k^2 E(k) at each output time.  With ref_n > 0 also the time series of kinetic
+    energy and dissipation of both GPU paths against the reference CPU run at ref_n^3."""
+    import math
+    import multiprocessing as mp
+    import numpy as np
+    import torch
+    from ns3d_wcns_b200 import analysis
+    from ns3d_wcns_b200.initial import isotropic_state
+    from ns3d_wcns_b200.solver import Solver
+    out = {}
+    pool, fut = None, None
+    if ref_n:
+        outs = [round(series_dt * (i + 1), 10) for i in range(int(round(max(t_outs) / series_dt)))]
+        pool = mp.get_context("spawn").Pool(1)
+        fut = pool.apply_async(_ref_series, ((ref_n, outs, 3, 2),))
+    fdev = f"cuda:{device}"
+    mu0, S = 1.0 / 400.0, 110.4 / 273.15
+
+    def run(n, precision, outs, keep):
+        P, G = bench_params(n, precision)
+        dV = (2 * math.pi / n) ** 3
+        s = Solver(P, G, device=device)
+        s.set_interior_primitives(*isotropic_state((n, n, n), 1.4, 0.3, seed=0))
+        log, snaps, t, steps = [], {}, 0.0, 0
+        t0 = time.perf_counter()
+
+        def step(t, t_out):
+            return s.time_advance(t_out, 1, t)[0]
+
+        for t_out in outs:
+            t = _advance_logged(step, t, t_out, s.total_energy, log)
+            W = _interior(s.primitives())
+            E = _interior(s.conserved()[4]) if keep is not None else None
+            T = _interior(s.temperature())
+            st = analysis.turbulence_stats(W[0], W[1], W[2], W[3], T, mu0, S, dV, device=fdev)
+            snap = {"stats": st}
+            if keep is not None:
+                snap["fields"] = {"rho": W[0], "u": W[1], "v": W[2], "w": W[3], "E": E}
+            snaps[t_out] = snap
+            del W, T, E
+        s.close()
+        return {"log": log, "snaps": snaps, "wall_s": time.perf_counter() - t0}
+
+    for n in sizes:
+        ref = run(n, 0, t_outs, keep=True)
+        mix = run(n, 1, t_outs, keep=True)
+        rows = {}
+        for t_out in t_outs:
+            a, b = mix["snaps"][t_out], ref["snaps"][t_out]
+            k = slice(1, n // 3 + 1)
+            rows[str(t_out)] = {
+                **{f"l2_{q}": analysis.rel_l2(a["fields"][q], b["fields"][q]) for q in ("rho", "u", "v", "w", "E")},
+                "l2_spectrum_k1_N3": analysis.rel_l2(a["stats"]["spectrum"][k], b["stats"]["spectrum"][k]),
+                "rel_total_energy": abs(a["stats"]["total_energy"] / b["stats"]["total_energy"] - 1),
+                "rel_dissipation": abs(a["stats"]["dissipation"] / b["stats"]["dissipation"] - 1),
+                "fp64_total_energy": b["stats"]["total_energy"], "fp64_dissipation": b["stats"]["dissipation"],
+            }
+        out[f"{n}^3"] = {"mixed_vs_fp64": rows, "steps_fp64": len(ref["log"]), "steps_mixed": len(mix["log"]),
+                         "wall_s_fp64": ref["wall_s"], "wall_s_mixed": mix["wall_s"]}
+        del ref, mix
+        torch.cuda.empty_cache()
+
+    if ref_n:
+        outs = [round(series_dt * (i + 1), 10) for i in range(int(round(max(t_outs) / series_dt)))]
+        gpu = {p: run(ref_n, p, outs, keep=None) for p in (0, 1)}
+        r = fut.get()
+        pool.close()
+        series = []
+        for t_out in outs:
+            row = {"t": t_out, "ref_total_energy": r["stats"][t_out]["total_energy"],
+                   "ref_dissipation": r["stats"][t_out]["dissipation"]}
+            for p, name in ((0, "fp64"), (1, "mixed")):
+                st = gpu[p]["snaps"][t_out]["stats"]
+                row[f"{name}_rel_total_energy"] = abs(st["total_energy"] / row["ref_total_energy"] - 1)
+                row[f"{name}_rel_dissipation"] = abs(st["dissipation"] / row["ref_dissipation"] - 1)
+            series.append(row)
+        # per-step kinetic energy along the whole run (same dt schedule when the steps agree)
+        steps = min(len(r["log"]), len(gpu[0]["log"]))
+        ke_fp64 = max(abs(gpu[0]["log"][i][1] / r["log"][i][1] - 1) for i in range(steps))
+        out[f"reference_{ref_n}^3"] = {"kind": r["kind"], "series": series, "steps_ref": len(r["log"]),
+                                       "steps_fp64": len(gpu[0]["log"]), "steps_mixed": len(gpu[1]["log"]),
+                                       "max_rel_ke_fp64_per_step": ke_fp64}
+    return out
+
+
 # --------------------------------------------------------------- GPU arm
 
 def main():
@@ -292,6 +431,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batch-problems", type=int, default=512)
+    ap.add_argument("--accuracy", default="", help="comma-separated grid sizes: accuracy report only")
+    ap.add_argument("--accuracy-ref", type=int, default=0, help="also the reference CPU time series at this size")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("NS3D_BENCH_ALLOW_SHORT"), \
         "at least 3 warm-up steps"
@@ -301,6 +442,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.accuracy:
+        rep = accuracy_report(local, sizes=[int(x) for x in args.accuracy.split(",")], ref_n=args.accuracy_ref)
+        print(json.dumps({"accuracy": rep}))
         return
 
     import numpy as np
