@@ -108,17 +108,25 @@ NS3D_HD R mdcd_hybrid(const R *lin, const R *hd, R f0, R f1, R f2, R f3, R f4, R
     t = f2 - R(2) * f3 + f4; u = R(3) * f2 - R(4) * f3 + f4;
     R be2 = c13 * (t * t) + R(0.25) * (u * u);
     R be3 = mdcd_beta3(f0, f1, f2, f3, f4, f5);
-    R tau6 = fabs(be3 - (be0 + R(4) * be1 + be2) / R(6));
-    R g0 = R(20) + tau6 / (be0 + eps_small);
-    R g1 = R(20) + tau6 / (be1 + eps_small);
-    R g2 = R(20) + tau6 / (be2 + eps_small);
-    R g3 = R(20) + tau6 / (be3 + eps_small);
-    R al0 = hd[0] * (g0 * g0), al1 = hd[1] * (g1 * g1), al2 = hd[2] * (g2 * g2), al3 = hd[3] * (g3 * g3);
     R q0 = R(3) * f0 - R(10) * f1 + R(15) * f2;
     R q1 = -f1 + R(6) * f2 + R(3) * f3;
     R q2 = R(3) * f2 + R(6) * f3 - f4;
     R q3 = R(15) * f3 - R(10) * f4 + R(3) * f5;
-    return (al0 * q0 + al1 * q1 + al2 * q2 + al3 * q3) / (R(8) * (al0 + al1 + al2 + al3));
+    // The weights d (20 + tau6/(beta + 1e-40))^2 span far more than the FP32
+    // range: FP32 inputs quantise a smooth stencil to beta == 0 exactly, and
+    // (tau6 * 1e40)^2 overflows to inf (inf/inf = NaN).  So the FP32 build
+    // forms the weights and the normalisation in FP64, like the reference;
+    // this branch is the rare one (most faces take the linear scheme above).
+    using Wt = double;
+    Wt tau6 = fabs((Wt)be3 - ((Wt)be0 + Wt(4) * (Wt)be1 + (Wt)be2) / Wt(6));
+    const Wt es = sizeof(R) == 8 ? (Wt)eps_small : Wt(1e-40);
+    Wt g0 = Wt(20) + tau6 / ((Wt)be0 + es);
+    Wt g1 = Wt(20) + tau6 / ((Wt)be1 + es);
+    Wt g2 = Wt(20) + tau6 / ((Wt)be2 + es);
+    Wt g3 = Wt(20) + tau6 / ((Wt)be3 + es);
+    Wt al0 = (Wt)hd[0] * (g0 * g0), al1 = (Wt)hd[1] * (g1 * g1), al2 = (Wt)hd[2] * (g2 * g2),
+       al3 = (Wt)hd[3] * (g3 * g3);
+    return (R)((al0 * (Wt)q0 + al1 * (Wt)q1 + al2 * (Wt)q2 + al3 * (Wt)q3) / (Wt(8) * (al0 + al1 + al2 + al3)));
 }
 
 // interpolate_select, interpolation.cpp:13-77, for the left state (flag +1,
