@@ -300,7 +300,8 @@ SweepArgs<R> sweep_args(ns3d_handle *h, int dir) {
     a.outflow_lo = h->P.bc[2 * dir] == NS3D_OUTFLOW;
     a.outflow_hi = h->P.bc[2 * dir + 1] == NS3D_OUTFLOW;
     a.inv_h = (R)(dir == 0 ? h->ph.inv_dx : dir == 1 ? h->ph.inv_dy : h->ph.inv_dz);
-    a.h = (R)(dir == 0 ? h->ph.dx : dir == 1 ? h->ph.dy : h->ph.dz);
+    const double hd = dir == 0 ? h->ph.dx : dir == 1 ? h->ph.dy : h->ph.dz;
+    a.dinv[0] = (R)(1.0 / (2.0 * hd)); a.dinv[1] = (R)(1.0 / (12.0 * hd)); a.dinv[2] = (R)(1.0 / (60.0 * hd));
     if constexpr (sizeof(R) == 8) a.sp = h->sp64; else a.sp = h->sp32;
     a.first = dir == 0;
     a.visc = h->ph.mu != 0.0;

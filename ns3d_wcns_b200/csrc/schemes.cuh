@@ -85,19 +85,30 @@ NS3D_HD float mdcd_beta3(float f0, float f1, float f2, float f3, float f4, float
     return q * (1.f / 120960.f) + f0 * f0 * (1.f / 6048.f);
 }
 
-// mdcd_hybrid_interpolate, interpolation.cpp:135-209.  The detector test
-// min(sai1, sai2) > 0.4 is evaluated as two cross-multiplied comparisons
-// (denominators are positive).
+// mdcd_hybrid_interpolate, interpolation.cpp:135-209, split into its
+// detector and its WENO branch.
+//
+// Detector: with a_j = |f_j - f_{j-1}| + |f_j - 2 f_{j-1} + f_{j-2}| and
+// b_j = |f_j - f_{j+1}| + |f_j - 2 f_{j+1} + f_{j+2}| at the two central
+// points j = 2, 3 of the stencil, the linear scheme is used when
+// min(sai(a_2, b_2), sai(a_3, b_3)) > 0.4 with sai(a, b) = (2ab + eps)/(a^2 +
+// b^2 + eps), evaluated as cross-multiplied comparisons (the denominators are
+// positive).  sai is symmetric in (a, b), and the reversed stencil of the
+// right state swaps a_j and b_j of the same two points with the same
+// operation order, so both states of a face take the same decision:
+// smooth(cell i) && smooth(cell i+1) for the face i+1/2.
 template <typename R>
-NS3D_HD R mdcd_hybrid(const R *lin, const R *hd, R f0, R f1, R f2, R f3, R f4, R f5) {
+NS3D_HD bool mdcd_smooth(R fm2, R fm1, R f0, R fp1, R fp2) {
     const R eps = R(0.9 * 0.4 / (1.0 - 0.9 * 0.4) * 1e-4);
-    R a1 = fabs(f2 - f1) + fabs(f2 - R(2) * f1 + f0);
-    R b1 = fabs(f2 - f3) + fabs(f2 - R(2) * f3 + f4);
-    R a2 = fabs(f3 - f2) + fabs(f3 - R(2) * f2 + f1);
-    R b2 = fabs(f3 - f4) + fabs(f3 - R(2) * f4 + f5);
-    bool s1 = (R(2) * a1 * b1 + eps) > R(0.4) * (a1 * a1 + b1 * b1 + eps);
-    bool s2 = (R(2) * a2 * b2 + eps) > R(0.4) * (a2 * a2 + b2 * b2 + eps);
-    if (s1 && s2) return mdcd_linear(lin, f0, f1, f2, f3, f4, f5);
+    R a = fabs(f0 - fm1) + fabs(f0 - R(2) * fm1 + fm2);
+    R b = fabs(f0 - fp1) + fabs(f0 - R(2) * fp1 + fp2);
+    return (R(2) * a * b + eps) > R(0.4) * (a * a + b * b + eps);
+}
+
+// The non-linear branch: 4-stencil WENO with weights d_k (20 + tau6/(beta_k +
+// 1e-40))^2 (interpolation.cpp:170-208).
+template <typename R>
+NS3D_HD R mdcd_weno_branch(const R *hd, R f0, R f1, R f2, R f3, R f4, R f5) {
     const R eps_small = sizeof(R) == 8 ? R(1e-40) : R(1e-40f);
     const R c13 = R(13.0 / 12.0);
     R t, u;
@@ -112,11 +123,11 @@ NS3D_HD R mdcd_hybrid(const R *lin, const R *hd, R f0, R f1, R f2, R f3, R f4, R
     R q1 = -f1 + R(6) * f2 + R(3) * f3;
     R q2 = R(3) * f2 + R(6) * f3 - f4;
     R q3 = R(15) * f3 - R(10) * f4 + R(3) * f5;
-    // The weights d (20 + tau6/(beta + 1e-40))^2 span far more than the FP32
-    // range: FP32 inputs quantise a smooth stencil to beta == 0 exactly, and
-    // (tau6 * 1e40)^2 overflows to inf (inf/inf = NaN).  So the FP32 build
-    // forms the weights and the normalisation in FP64, like the reference;
-    // this branch is the rare one (most faces take the linear scheme above).
+    // The weights span far more than the FP32 range: FP32 inputs quantise a
+    // smooth stencil to beta == 0 exactly, and (tau6 * 1e40)^2 overflows to
+    // inf (inf/inf = NaN).  So the FP32 build forms the weights and the
+    // normalisation in FP64, like the reference; this branch is the rare one
+    // (most faces take the linear scheme).
     using Wt = double;
     Wt tau6 = fabs((Wt)be3 - ((Wt)be0 + Wt(4) * (Wt)be1 + (Wt)be2) / Wt(6));
     const Wt es = sizeof(R) == 8 ? (Wt)eps_small : Wt(1e-40);
@@ -127,6 +138,13 @@ NS3D_HD R mdcd_hybrid(const R *lin, const R *hd, R f0, R f1, R f2, R f3, R f4, R
     Wt al0 = (Wt)hd[0] * (g0 * g0), al1 = (Wt)hd[1] * (g1 * g1), al2 = (Wt)hd[2] * (g2 * g2),
        al3 = (Wt)hd[3] * (g3 * g3);
     return (R)((al0 * (Wt)q0 + al1 * (Wt)q1 + al2 * (Wt)q2 + al3 * (Wt)q3) / (Wt(8) * (al0 + al1 + al2 + al3)));
+}
+
+template <typename R>
+NS3D_HD R mdcd_hybrid(const R *lin, const R *hd, R f0, R f1, R f2, R f3, R f4, R f5) {
+    if (mdcd_smooth(f0, f1, f2, f3, f4) && mdcd_smooth(f1, f2, f3, f4, f5))
+        return mdcd_linear(lin, f0, f1, f2, f3, f4, f5);
+    return mdcd_weno_branch(hd, f0, f1, f2, f3, f4, f5);
 }
 
 // interpolate_select, interpolation.cpp:13-77, for the left state (flag +1,
@@ -140,6 +158,27 @@ NS3D_HD R interp_side(const SchemeParams<R> &sp, const R *f, bool right) {
     if (it == I_WENO5) return weno5(g0, g1, g2, g3, g4);
     if (it == I_MDCD_LINEAR) return mdcd_linear(sp.lin, g0, g1, g2, g3, g4, g5);
     return mdcd_hybrid(sp.lin, sp.hd, g0, g1, g2, g3, g4, g5);
+}
+
+// Left and right states of one conserved variable at face i+1/2 from the
+// stencil f[0..5] = cells i-2 .. i+3 (component-wise interpolation).  For
+// MDCD_HYBRID the detector is evaluated once for both sides (see
+// mdcd_smooth); every value equals interp_side's.
+template <typename R, int INTERP>
+NS3D_HD void face_pair(const SchemeParams<R> &sp, const R *f, R &L, R &Rr) {
+    const int it = INTERP == RUNTIME ? sp.interp : INTERP;
+    if (it == I_MDCD_HYBRID) {
+        if (mdcd_smooth(f[0], f[1], f[2], f[3], f[4]) && mdcd_smooth(f[1], f[2], f[3], f[4], f[5])) {
+            L = mdcd_linear(sp.lin, f[0], f[1], f[2], f[3], f[4], f[5]);
+            Rr = mdcd_linear(sp.lin, f[5], f[4], f[3], f[2], f[1], f[0]);
+        } else {
+            L = mdcd_weno_branch(sp.hd, f[0], f[1], f[2], f[3], f[4], f[5]);
+            Rr = mdcd_weno_branch(sp.hd, f[5], f[4], f[3], f[2], f[1], f[0]);
+        }
+        return;
+    }
+    L = interp_side<R, INTERP>(sp, f, false);
+    Rr = interp_side<R, INTERP>(sp, f, true);
 }
 
 // ------------------------------------------------------------ Riemann solvers
@@ -201,9 +240,12 @@ NS3D_HD void roe_flux(const R *UL, const R *UR, R g, R *F) {
     R A4 = (t - s) * i2c2;   // acoustic wave V + c
     R l0 = fabs(V - c), lv = fabs(V), l4 = fabs(V + c);
     R delta = R(0.1) * (lv + c);
-    if (l0 < delta) l0 = (l0 * l0 + delta * delta) / (R(2) * delta);
-    if (lv < delta) lv = (lv * lv + delta * delta) / (R(2) * delta);
-    if (l4 < delta) l4 = (l4 * l4 + delta * delta) / (R(2) * delta);
+    // (l^2 + delta^2) / (2 delta) below delta, through one reciprocal and
+    // selects (no divergent division per eigenvalue)
+    const R i2d = R(1) / (R(2) * delta), d2 = delta * delta;
+    l0 = l0 < delta ? (l0 * l0 + d2) * i2d : l0;
+    lv = lv < delta ? (lv * lv + d2) * i2d : lv;
+    l4 = l4 < delta ? (l4 * l4 + d2) * i2d : l4;
     R k0 = (l0 - lv) * A0, k4 = (l4 - lv) * A4;
     // R0 = (1, u-nc, v-nc, w-nc, H-cV), R4 = (1, u+nc, v+nc, w+nc, H+cV)
     R cx = DIR == 0 ? c : R(0), cy = DIR == 1 ? c : R(0), cz = DIR == 2 ? c : R(0);
@@ -290,9 +332,19 @@ NS3D_HD void hllc_flux(const R *UL, const R *UR, R g, R *F) {
         R sL = sqrt(L.r), sR = sqrt(Rt.r);
         SM = (sL * L.un + sR * Rt.un) / (sL + sR);
     }
+    // the star state of the upwind side: selected, not branched, so faces of
+    // one warp with different signs of S_M do not diverge
+    const bool left = SM >= R(0);
+    Side<DIR, R> S;
+    S.r = left ? L.r : Rt.r; S.ir = left ? L.ir : Rt.ir;
+    S.u = left ? L.u : Rt.u; S.v = left ? L.v : Rt.v; S.w = left ? L.w : Rt.w;
+    S.E = left ? L.E : Rt.E; S.p = left ? L.p : Rt.p; S.un = left ? L.un : Rt.un;
+    R Us[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) Us[n] = left ? UL[n] : UR[n];
     R Fs[5];
-    if (SM >= R(0)) { L.flux(Fs); hllc_star<DIR, R>(L, UL, Fs, SL, SM, F); }
-    else { Rt.flux(Fs); hllc_star<DIR, R>(Rt, UR, Fs, SR, SM, F); }
+    S.flux(Fs);
+    hllc_star<DIR, R>(S, Us, Fs, left ? SL : SR, SM, F);
 }
 
 // HLLC_p_Riemann_solver, InviscousFlux.cpp:594-717: PVRS p*, Toro speeds.
@@ -421,10 +473,7 @@ NS3D_HD void wcns_face(const SchemeParams<R> &sp, const R U[5][6], const R *wi,
     const bool ch = CHAR == RUNTIME ? (sp.char_recon != 0) : (CHAR != 0);
     if (!ch) {
 #pragma unroll
-        for (int n = 0; n < 5; ++n) {
-            UL[n] = interp_side<R, INTERP>(sp, U[n], false);
-            UR[n] = interp_side<R, INTERP>(sp, U[n], true);
-        }
+        for (int n = 0; n < 5; ++n) face_pair<R, INTERP>(sp, U[n], UL[n], UR[n]);
     } else if (CHAR != 0) {
         R Lm[5][5], Rm[5][5], Q[5], Wc[6];
 #pragma unroll 1

@@ -13,10 +13,10 @@
 //
 // A thread block owns a bundle of lines and marches along them in chunks of C
 // faces.  Conserved cells, viscous node fluxes and face fluxes live in
-// shared-memory rings, so each cell is loaded and converted once and each face
-// flux is computed once per line (plus a 5-face halo at the line ends).  The
-// next chunk's cells and viscous fluxes, and the current chunk's old RHS
-// values, are copied with cp.async while the face fluxes compute.  In periodic
+// chunk-relative shared-memory buffers, so each cell is loaded and converted
+// once and each face flux is computed once per line (plus a 5-face halo at
+// the line ends).  The next chunk's cells and viscous fluxes are copied with
+// cp.async, and the old RHS values loaded, while the face fluxes compute.  In periodic
 // directions the wrapped faces are computed from wrapped cells (identical
 // inputs, identical values to the reference's face exchange); in non-periodic
 // directions the ghost faces are the Outflow copies or zero, as the reference
@@ -43,32 +43,51 @@ struct SweepArgs {
     int periodic;       // this direction
     int outflow_lo, outflow_hi;  // ghost faces copy the boundary face (else zero)
     R inv_h;            // 1/h of this direction
-    R h;                // h (viscous stencils divide by k*h as the reference)
+    R dinv[3];          // 1/(2h), 1/(12h), 1/(60h): the viscous stencils' divisors
     SchemeParams<R> sp;
     int first;          // 1: write (first direction), 0: accumulate
     int visc;           // 1: add the viscous divergence term
 };
 
+// Chunk geometry.  A chunk holds C faces of every line of the block.  Its
+// shared-memory buffers are indexed relative to the chunk (no ring wrap):
+//   cells  position p <-> cell fc - 2 + p, p in [0, NU)  (conserved state)
+//   faces  position p <-> face fc - 5 + p, p in [0, NF)
+//   visc   position p <-> cell fc - 5 + p, p in [0, NV)  (node fluxes)
+// At the end of a chunk the tails are moved to the front and the staged next
+// cells appended, so every stencil read is a fixed offset from the thread's
+// own position.
 template <int DIR>
 struct SweepGeom {
     static constexpr int C = DIR == 0 ? 32 : 8;        // faces per chunk
     static constexpr int NLINE = DIR == 0 ? 8 : 32;    // lines per block
-    static constexpr int RING = DIR == 0 ? 64 : 16;    // ring length (power of 2, >= C+8)
-    static constexpr int SIZE = NLINE * RING;
-    static constexpr int CH = C * NLINE;               // cells per chunk = threads
-    __device__ __forceinline__ static int sidx(int line, int r) {
-        return DIR == 0 ? line * RING + (r & (RING - 1)) : (r & (RING - 1)) * NLINE + line;
+    static constexpr int CH = C * NLINE;               // threads
+    static constexpr int NU = C + 5, NF = C + 7, NV = C + 8;
+    // along x a warp owns one line ([line][pos]); along y/z the lanes span 32
+    // neighbouring lines ([pos][line]); both are conflict-free
+    template <int NP>
+    __device__ __forceinline__ static int idx(int line, int pos) {
+        return DIR == 0 ? line * NP + pos : pos * NLINE + line;
     }
     __device__ __forceinline__ static int tidx(int line, int slot) {
         return DIR == 0 ? line * C + slot : slot * NLINE + line;
     }
 };
 
-// rings U(5) F(5) V(4) [W(5) with characteristic bases], staging W(5)+V(4), old RHS(5)
+// The old RHS of the updated cell is staged in shared memory with the next
+// chunk's cells (true) or loaded into registers (false).
+constexpr bool kRoldSmem = true;
+// minimum resident blocks per SM requested from the register allocator
+template <typename R>
+constexpr int sweep_min_blocks() { return 2; }
+
+// buffers U(5) F(5) V(4) [W(5) for characteristic bases], staging W(5)+V(4)
+// [+ old RHS(5)]
 template <int DIR, typename R, bool CHARW>
 constexpr size_t sweep_smem_bytes() {
     using G = SweepGeom<DIR>;
-    return sizeof(R) * ((size_t)(14 + (CHARW ? 5 : 0)) * G::SIZE + (size_t)14 * G::CH);
+    return sizeof(R) * ((size_t)G::NLINE * (5 * G::NU + 5 * G::NF + 4 * G::NV + (CHARW ? 5 * G::NU : 0)) +
+                        (size_t)(kRoldSmem ? 14 : 9) * G::CH);
 }
 
 template <typename R>
@@ -80,203 +99,308 @@ __device__ __forceinline__ void to_conserved(const SweepArgs<R> &a, R r, R u, R 
     }
 }
 
+// first derivative along the line, ViscousFlux.cpp:15-29 with the order of
+// choose_scheme; dinv = 1/(2h), 1/(12h), 1/(60h).  Order -1 reproduces the
+// reference's backward form, which evaluates to -df/dx.
+template <typename R, typename F>
+__device__ __forceinline__ R dstencil_inv(F f, int order, const R *dinv) {
+    if (order == 6)
+        return (f(3) - R(9) * f(2) + R(45) * f(1) - R(45) * f(-1) + R(9) * f(-2) - f(-3)) * dinv[2];
+    if (order == 1 || order == -1) return (R(-3) * f(0) + R(4) * f(order) - f(2 * order)) * dinv[0];
+    if (order == 2) return (f(1) - f(-1)) * dinv[0];
+    return (-f(2) + R(8) * f(1) - R(8) * f(-1) + f(-2)) * dinv[1];
+}
+
 template <int DIR, typename R, int INTERP, int RS, int CHAR>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sweep_min_blocks<R>())
 sweep_kernel(SweepArgs<R> a) {
     using G = SweepGeom<DIR>;
-    constexpr int C = G::C, SZ = G::SIZE, CH = G::CH;
+    constexpr int C = G::C, NL = G::NLINE, CH = G::CH, NU = G::NU, NF = G::NF, NV = G::NV;
     constexpr bool USE_W = (CHAR != 0);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R *base = reinterpret_cast<R *>(smem_raw);
-    R (*sU)[SZ] = reinterpret_cast<R (*)[SZ]>(base);
-    R (*sF)[SZ] = sU + 5;
-    R (*sV)[SZ] = sU + 10;
-    R (*sW)[SZ] = sU + 14;  // characteristic bases only
-    R (*stg)[CH] = reinterpret_cast<R (*)[CH]>(base + (14 + (USE_W ? 5 : 0)) * SZ);  // [9][CH]
-    R (*rold)[CH] = stg + 9;                                                          // [5][CH]
+    R *const sU = reinterpret_cast<R *>(smem_raw);  // [5][NL*NU]
+    R *const sF = sU + 5 * NL * NU;                  // [5][NL*NF]
+    R *const sV = sF + 5 * NL * NF;                  // [4][NL*NV]
+    R *const sW = sV + 4 * NL * NV;                  // [5][NL*NU] characteristic bases only
+    R *const stg = sW + (USE_W ? 5 * NL * NU : 0);   // [9][CH]
+    R *const srold = stg + 9 * CH;                   // [5][CH] (kRoldSmem)
 
     const Layout &L = a.L;
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int line = DIR == 0 ? threadIdx.y : threadIdx.x;
-    int ta = blockIdx.x * G::NLINE + line, tb = blockIdx.y;
-    const bool line_ok = ta < (DIR == 0 ? L.ny : L.nx);
-    ta += NG; tb += NG;
+    const int ta0 = blockIdx.x * NL + line, tb0 = blockIdx.y;
+    const bool line_ok = ta0 < (DIR == 0 ? L.ny : L.nx);
     const int n = DIR == 0 ? L.nx : (DIR == 1 ? L.ny : L.nz);
-    auto cell_id = [&](int c) -> long {
-        if (DIR == 0) return L.at(c, ta, tb);
-        if (DIR == 1) return L.at(ta, c, tb);
-        return L.at(ta, tb, c);
-    };
-    // interior-layout index of interior position ci along the line
-    auto vis_id = [&](int ci) -> long {
-        const int a0 = ta - NG, b0 = tb - NG;
-        if (DIR == 0) return ((long)b0 * L.ny + a0) * L.nx + ci;
-        if (DIR == 1) return ((long)b0 * L.ny + ci) * L.nx + a0;
-        return ((long)ci * L.ny + b0) * L.nx + a0;
-    };
+    // padded-layout address of cell c (ghost-inclusive index along the line)
+    long lbase, lstride, vbase, vstride;
+    if (DIR == 0) {
+        lbase = L.at(0, ta0 + NG, tb0 + NG); lstride = 1;
+        vbase = ((long)tb0 * L.ny + ta0) * L.nx; vstride = 1;
+    } else if (DIR == 1) {
+        lbase = L.at(ta0 + NG, 0, tb0 + NG); lstride = L.px;
+        vbase = (long)tb0 * L.ny * L.nx + ta0; vstride = L.nx;
+    } else {
+        lbase = L.at(ta0 + NG, tb0 + NG, 0); lstride = (long)L.px * L.sy;
+        vbase = (long)tb0 * L.nx + ta0; vstride = (long)L.nx * L.ny;
+    }
     const bool per = a.periodic != 0;
     const bool visc = a.visc != 0;
     const bool rmw = a.first == 0;
     const int fb = per ? 0 : NG - 1;           // first face computed from cells
-    const int fe = per ? n + 5 : n + NG;       // one past the last
+    const int fe = per ? n + 5 : n + NG;       // one past the last computed face
     const int cell_end = per ? n + 8 : n + 6;  // one past the last cell needed
+    const int chunk_end = n + NG + 2;          // chunks run while fc - 2 < n + NG
     const bool char_rt = CHAR == RUNTIME ? (a.sp.char_recon != 0) : (CHAR != 0);
     const int ti = G::tidx(line, slot);
 
     auto wrap = [&](int c) { return per ? (c < NG ? c + n : (c >= n + NG ? c - n : c)) : c; };
-    // interior index of the viscous node flux of cell c; -1 outside a
-    // non-periodic interior (never read there: the orders stay inside)
+    // interior index of the node flux of cell c, or -1 (outside a
+    // non-periodic interior, or before the first needed cell: never read)
     auto vis_pos = [&](int c) -> int {
+        if (c < 0) return -1;
         int ci = c - NG;
         if (per) { if (ci < 0) ci += n; else if (ci >= n) ci -= n; return ci; }
         return (ci >= 0 && ci < n) ? ci : -1;
     };
-    // one converted cell into the rings
-    auto put_cell = [&](int c, R r, R u, R v, R w, R p, const R *vf) {
+    auto put_cell = [&](int pu, int pv, R r, R u, R v, R w, R p, const R *vf) {
         R U[5];
         to_conserved(a, r, u, v, w, p, U);
-        const int s = G::sidx(line, c);
+        const int s = G::template idx<NU>(line, pu);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) sU[q][s] = U[q];
+        for (int q = 0; q < 5; ++q) sU[q * NL * NU + s] = U[q];
         if (USE_W && char_rt) {
-            sW[0][s] = r <= R(0) ? R(1e-12) : r; sW[1][s] = u; sW[2][s] = v; sW[3][s] = w; sW[4][s] = p;
+            R *w5 = sW + s;
+            w5[0] = r <= R(0) ? R(1e-12) : r; w5[NL * NU] = u; w5[2 * NL * NU] = v;
+            w5[3 * NL * NU] = w; w5[4 * NL * NU] = p;
         }
-        if (visc) {
+        if (visc && pv >= 0) {
+            const int sv = G::template idx<NV>(line, pv);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) sV[q][s] = vf[q];
-        }
-    };
-    // asynchronous staging of cell c (primitives + viscous fluxes)
-    auto stage_cell = [&](int c) {
-        const long id = cell_id(wrap(c));
-#pragma unroll
-        for (int q = 0; q < 5; ++q) cp_async(&stg[q][ti], a.W[q] + id);
-        if (visc) {
-            const int ci = vis_pos(c);
-            if (ci >= 0) {
-                const long vid = vis_id(ci);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) cp_async(&stg[5 + q][ti], a.V[q] + vid);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) stg[5 + q][ti] = R(0);
-            }
+            for (int q = 0; q < 4; ++q) sV[q * NL * NV + sv] = vf[q];
         }
     };
 
-    // ---- first chunk: the cells of faces [fb, fb+C) are loaded directly
-    int loaded = fb - 2;
-    {
-        const int need = min(fb + C + 3, cell_end);
-        for (int c = loaded + slot; c < need; c += C) {
-            if (!line_ok) continue;
-            const long id = cell_id(wrap(c));
+    // ---- first chunk: visc positions [0, NV) = cells fb-5 .., cell
+    //      positions [0, NU) = cells fb-2 .. (position p-3 of the same cell)
+    if (line_ok) {
+        for (int p = slot; p < NV; p += C) {
+            const int c = fb - 5 + p;
             R vf[4] = {R(0), R(0), R(0), R(0)};
             if (visc) {
                 const int ci = vis_pos(c);
                 if (ci >= 0) {
-                    const long vid = vis_id(ci);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) vf[q] = a.V[q][vid];
+                    for (int q = 0; q < 4; ++q) vf[q] = a.V[q][vbase + ci * vstride];
                 }
             }
-            put_cell(c, a.W[0][id], a.W[1][id], a.W[2][id], a.W[3][id], a.W[4][id], vf);
+            if (p >= 3 && c < cell_end) {
+                const long id = lbase + wrap(c) * lstride;
+                put_cell(p - 3, p, a.W[0][id], a.W[1][id], a.W[2][id], a.W[3][id], a.W[4][id], vf);
+            } else if (visc) {
+                const int sv = G::template idx<NV>(line, p);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) sV[q * NL * NV + sv] = vf[q];
+            }
         }
-        loaded = need;
     }
 
-    for (int fc = fb; fc < fe; fc += C) {
-        const bool last = fc + C >= fe;
-        const int c_hi = last ? n + NG : min(fc + C - 2, n + NG);
-        // ---- asynchronous fetches: the old RHS of this slot's first cell
-        //      (group 1) and the next chunk's new cell (group 2)
-        const int rc = fc - 2 + slot;
-        if (rmw && line_ok && rc >= NG && rc < c_hi) {
-            const long id = cell_id(rc);
+    for (int fc = fb; fc < chunk_end; fc += C) {
+        // cell updated by this thread in this chunk; its old RHS (plain
+        // loads, consumed after the face phase)
+        const int cu = fc - 2 + slot;
+        const bool upd = line_ok && cu >= NG && cu < n + NG;
+        const long cid = lbase + cu * lstride;
+        R rold[5];
 #pragma unroll
-            for (int q = 0; q < 5; ++q) cp_async(&rold[q][ti], a.Rhs[q] + id);
+        for (int q = 0; q < 5; ++q) rold[q] = R(0);
+        if (rmw && upd) {
+            if constexpr (kRoldSmem) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) cp_async(&srold[q * CH + ti], a.Rhs[q] + cid);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) rold[q] = a.Rhs[q][cid];
+            }
+        }
+        if constexpr (kRoldSmem) cp_async_commit();
+        // stage the next chunk's new cell (cell and visc positions 5+slot, 8+slot)
+        const int cn = fc + C + 3 + slot;
+        const bool stage = fc + C < chunk_end && line_ok && cn < cell_end;
+        if (stage) {
+            const long id = lbase + wrap(cn) * lstride;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) cp_async(&stg[q * CH + ti], a.W[q] + id);
+            if (visc) {
+                const int ci = vis_pos(cn);
+                if (ci >= 0) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) cp_async(&stg[(5 + q) * CH + ti], a.V[q] + vbase + ci * vstride);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) stg[(5 + q) * CH + ti] = R(0);
+                }
+            }
         }
         cp_async_commit();
-        const int nfc = fc + C;
-        const int next_need = min(nfc + C + 3, cell_end);
-        const int pc = loaded + slot;
-        const bool prefetch = nfc < fe && line_ok && pc < next_need;
-        if (prefetch) stage_cell(pc);
-        cp_async_commit();
-        __syncthreads();  // rings of this chunk complete
-        // ---- face flux of face f (between cells f and f+1): cells f-2 .. f+3
+        __syncthreads();  // buffers of this chunk complete
+
+        // ---- face f = fc + slot (between cells f and f+1): cell positions slot .. slot+5
         const int f = fc + slot;
-        if (line_ok && f < fe) {
+        if (CHAR == 0 && line_ok && f < fe) {
             R st[5][6];
 #pragma unroll
-            for (int m = 0; m < 6; ++m) {
-                const int s = G::sidx(line, f - 2 + m);
+            for (int q = 0; q < 5; ++q)
 #pragma unroll
-                for (int q = 0; q < 5; ++q) st[q][m] = sU[q][s];
+                for (int m = 0; m < 6; ++m) st[q][m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
+            R UL[5], UR[5];
+            if constexpr (INTERP == I_MDCD_HYBRID) {
+                // detector of every variable, the linear states of all, then
+                // the WENO branch only where a detector rejected the linear
+                // scheme (rare): the common path has no divergent branch
+                unsigned weno = 0;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    const bool lin = mdcd_smooth(st[q][0], st[q][1], st[q][2], st[q][3], st[q][4]) &&
+                                     mdcd_smooth(st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]);
+                    weno |= (lin ? 0u : 1u) << q;
+                    UL[q] = mdcd_linear(a.sp.lin, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]);
+                    UR[q] = mdcd_linear(a.sp.lin, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1], st[q][0]);
+                }
+                if (weno) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q)
+                        if (weno & (1u << q)) {
+                            UL[q] = mdcd_weno_branch(a.sp.hd, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]);
+                            UR[q] = mdcd_weno_branch(a.sp.hd, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1], st[q][0]);
+                        }
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) face_pair<R, INTERP>(a.sp, st[q], UL[q], UR[q]);
             }
+            R F[5];
+            riemann<DIR, R, RS>(a.sp, UL, UR, F);
+            const int s = G::template idx<NF>(line, slot + 5);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) sF[q * NL * NF + s] = F[q];
+        } else if (line_ok && f < fe) {
+            R st[5][6];
+#pragma unroll
+            for (int q = 0; q < 5; ++q)
+#pragma unroll
+                for (int m = 0; m < 6; ++m) st[q][m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
             R wi[5], wi1[5];
             if (USE_W && char_rt) {
-                const int s0 = G::sidx(line, f), s1 = G::sidx(line, f + 1);
+                const int s0 = G::template idx<NU>(line, slot + 2), s1 = G::template idx<NU>(line, slot + 3);
 #pragma unroll
-                for (int q = 0; q < 5; ++q) { wi[q] = sW[q][s0]; wi1[q] = sW[q][s1]; }
+                for (int q = 0; q < 5; ++q) { wi[q] = sW[q * NL * NU + s0]; wi1[q] = sW[q * NL * NU + s1]; }
             }
             R F[5];
             wcns_face<DIR, R, INTERP, RS, CHAR>(a.sp, st, wi, wi1, F);
-            const int s = G::sidx(line, f);
+            const int s = G::template idx<NF>(line, slot + 5);
 #pragma unroll
-            for (int q = 0; q < 5; ++q) sF[q][s] = F[q];
+            for (int q = 0; q < 5; ++q) sF[q * NL * NF + s] = F[q];
         }
-        cp_async_wait<1>();  // this thread's old-RHS copies have landed
-        __syncthreads();     // face fluxes complete
-        // ---- cells whose six faces (c-3 .. c+2) are now available
-        for (int c = rc; c < c_hi; c += C) {
-            if (!line_ok || c < NG) continue;
-            R fv[5][6];
+        if constexpr (kRoldSmem) cp_async_wait<1>();  // this thread's old-RHS copies landed
+        __syncthreads();  // faces of this chunk complete
+        if constexpr (kRoldSmem) {
+            if (rmw && upd) {
 #pragma unroll
-            for (int m = 0; m < 6; ++m) {
-                int ff = c - 3 + m;
-                bool zero = false;
-                if (!per) {
-                    if (ff < NG - 1) { if (a.outflow_lo) ff = NG - 1; else zero = true; }
-                    else if (ff > n + NG - 1) { if (a.outflow_hi) ff = n + NG - 1; else zero = true; }
+                for (int q = 0; q < 5; ++q) rold[q] = srold[q * CH + ti];
+            }
+        }
+
+        // ---- cell cu: faces cu-3 .. cu+2 at positions slot .. slot+5,
+        //      node fluxes cu-3 .. cu+3 at visc positions slot .. slot+6
+        if (upd) {
+            // within 3 cells of a non-periodic boundary the reference's ghost
+            // faces (Outflow copy of the boundary face, else zero) and the
+            // reduced viscous orders apply; everywhere else one straight path
+            const bool edge = !per && (cu - NG < 3 || cu - NG >= n - 3);
+            R d[5], vd[4] = {R(0), R(0), R(0), R(0)};
+            if (!edge) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    const R *fq = sF + q * NL * NF;
+                    auto F_ = [&](int m) { return fq[G::template idx<NF>(line, slot + m)]; };
+                    // diff_6th_central_half, InviscousFlux.cpp:990-992
+                    d[q] = ((F_(3) - F_(2)) * R(75.0 / 64.0) + (F_(4) - F_(1)) * R(-25.0 / 384.0) +
+                            (F_(5) - F_(0)) * R(3.0 / 640.0)) * a.inv_h;
                 }
-                const int s = G::sidx(line, ff);
+                if (visc) {
 #pragma unroll
-                for (int q = 0; q < 5; ++q) fv[q][m] = zero ? R(0) : sF[q][s];
+                    for (int q = 0; q < 4; ++q) {
+                        const R *vq = sV + q * NL * NV;
+                        auto V_ = [&](int off) { return vq[G::template idx<NV>(line, slot + 3 + off)]; };
+                        vd[q] = (V_(3) - R(9) * V_(2) + R(45) * V_(1) - R(45) * V_(-1) + R(9) * V_(-2) - V_(-3)) *
+                                a.dinv[2];
+                    }
+                }
+            } else {
+                const int pf_lo = (NG - 1) - (fc - 5), pf_hi = (n + NG - 1) - (fc - 5);
+#pragma unroll 1
+                for (int q = 0; q < 5; ++q) {
+                    R fv[6];
+                    for (int m = 0; m < 6; ++m) {
+                        int pm = slot + m;
+                        bool zero = false;
+                        const int ff = cu - 3 + m;
+                        if (ff < NG - 1) { if (a.outflow_lo) pm = pf_lo; else zero = true; }
+                        else if (ff > n + NG - 1) { if (a.outflow_hi) pm = pf_hi; else zero = true; }
+                        fv[m] = zero ? R(0) : sF[q * NL * NF + G::template idx<NF>(line, pm)];
+                    }
+                    d[q] = ((fv[3] - fv[2]) * R(75.0 / 64.0) + (fv[4] - fv[1]) * R(-25.0 / 384.0) +
+                            (fv[5] - fv[0]) * R(3.0 / 640.0)) * a.inv_h;
+                }
+                if (visc) {
+                    const int o = visc_order(cu - NG, n, false);
+#pragma unroll 1
+                    for (int q = 0; q < 4; ++q)
+                        vd[q] = dstencil_inv<R>(
+                            [&](int off) { return sV[q * NL * NV + G::template idx<NV>(line, slot + 3 + off)]; },
+                            o, a.dinv);
+                }
             }
-            R vd[4] = {R(0), R(0), R(0), R(0)};
-            if (visc) {
-                const int o = visc_order(c - NG, n, per);
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    vd[q] = dstencil<R>([&](int off) { return sV[q][G::sidx(line, c + off)]; }, o, a.h);
-            }
-            const long id = cell_id(c);
-            const bool staged = c == rc;
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                // diff_6th_central_half, InviscousFlux.cpp:990-992
-                R d = ((fv[q][3] - fv[q][2]) * R(75.0 / 64.0) + (fv[q][4] - fv[q][1]) * R(-25.0 / 384.0) +
-                       (fv[q][5] - fv[q][0]) * R(3.0 / 640.0)) * a.inv_h;
-                R old = R(0);
-                if (rmw) old = staged ? rold[q][ti] : a.Rhs[q][id];
-                R r = old - d;
+                R r = rold[q] - d[q];
                 if (q > 0) r += vd[q - 1];
-                a.Rhs[q][id] = r;
+                a.Rhs[q][cid] = r;
             }
         }
-        // ---- commit the staged next-chunk cell into the rings
         cp_async_wait<0>();
-        __syncthreads();  // staging complete; face-flux and ring reads of this chunk done
-        if (prefetch) {
-            R v4[4] = {R(0), R(0), R(0), R(0)};
-            if (visc) {
+        __syncthreads();  // buffer reads of this chunk done; staged cells landed
+
+        // ---- move the tails to the front, append the staged cell
+        if (line_ok && fc + C < chunk_end) {
+            if (visc && slot >= C - 8) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) v4[q] = stg[5 + q][ti];
+                for (int q = 0; q < 4; ++q)
+                    sV[q * NL * NV + G::template idx<NV>(line, slot - C + 8)] =
+                        sV[q * NL * NV + G::template idx<NV>(line, slot + 8)];
             }
-            put_cell(pc, stg[0][ti], stg[1][ti], stg[2][ti], stg[3][ti], stg[4][ti], v4);
+            if (slot >= C - 5) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    sU[q * NL * NU + G::template idx<NU>(line, slot - C + 5)] =
+                        sU[q * NL * NU + G::template idx<NU>(line, slot + 5)];
+                    sF[q * NL * NF + G::template idx<NF>(line, slot - C + 5)] =
+                        sF[q * NL * NF + G::template idx<NF>(line, slot + 5)];
+                    if (USE_W && char_rt)
+                        sW[q * NL * NU + G::template idx<NU>(line, slot - C + 5)] =
+                            sW[q * NL * NU + G::template idx<NU>(line, slot + 5)];
+                }
+            }
+            if (stage) {
+                R v4[4] = {R(0), R(0), R(0), R(0)};
+                if (visc) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) v4[q] = stg[(5 + q) * CH + ti];
+                }
+                put_cell(5 + slot, 8 + slot, stg[ti], stg[CH + ti], stg[2 * CH + ti], stg[3 * CH + ti],
+                         stg[4 * CH + ti], v4);
+            }
         }
-        loaded = next_need;
     }
 }
 
