@@ -323,6 +323,11 @@ ViscArgs<R> visc_args(ns3d_handle *h) {
     a.L = sizeof(R) == 8 ? h->L64 : h->L32;
     for (int d = 0; d < 3; ++d) a.periodic[d] = h->bc.periodic[d];
     a.h[0] = (R)h->ph.dx; a.h[1] = (R)h->ph.dy; a.h[2] = (R)h->ph.dz;
+    const double hh[3] = {h->ph.dx, h->ph.dy, h->ph.dz};
+    for (int d = 0; d < 3; ++d) {
+        a.dinv[d][0] = (R)(1.0 / (2.0 * hh[d])); a.dinv[d][1] = (R)(1.0 / (12.0 * hh[d]));
+        a.dinv[d][2] = (R)(1.0 / (60.0 * hh[d]));
+    }
     a.mu0 = (R)h->ph.mu; a.S = (R)h->ph.S;
     a.cp_over_pr = (R)(h->ph.Cp / h->ph.Pr);
     return a;
@@ -334,7 +339,7 @@ int rhs_impl(ns3d_handle *h) {
     cudaError_t e;
     if (h->ph.mu != 0.0) {  // Re = inf: the viscous terms are exactly zero
         ViscArgs<R> va = visc_args<R>(h);
-        dim3 g((va.L.nx + VTX - 1) / VTX, (va.L.ny + VTY - 1) / VTY, va.L.nz);
+        dim3 g((va.L.nx + VTX - 1) / VTX, (va.L.ny + VTY - 1) / VTY, (va.L.nz + VZC - 1) / VZC);
         prof_begin(h, "viscous_flux");
         viscous_flux_kernel<R><<<g, dim3(VTX, VTY), 0, st>>>(va);
         prof_end(h);

@@ -338,9 +338,10 @@ sweep_kernel(SweepArgs<R> a) {
                 }
             } else {
                 const int pf_lo = (NG - 1) - (fc - 5), pf_hi = (n + NG - 1) - (fc - 5);
-#pragma unroll 1
+#pragma unroll
                 for (int q = 0; q < 5; ++q) {
                     R fv[6];
+#pragma unroll
                     for (int m = 0; m < 6; ++m) {
                         int pm = slot + m;
                         bool zero = false;
@@ -354,7 +355,7 @@ sweep_kernel(SweepArgs<R> a) {
                 }
                 if (visc) {
                     const int o = visc_order(cu - NG, n, false);
-#pragma unroll 1
+#pragma unroll
                     for (int q = 0; q < 4; ++q)
                         vd[q] = dstencil_inv<R>(
                             [&](int off) { return sV[q * NL * NV + G::template idx<NV>(line, slot + 3 + off)]; },

@@ -8,10 +8,8 @@
 // (compute_viscous_flux, ViscousFlux.cpp:151-208; F_v = (txx,txy,txz,ex),
 // H_v = (txy,tyy,tyz,ey), G_v = (txz,tyz,tzz,ez)).
 //
-// A block owns a 32 x 8 tile of one z-plane: the tile and its 3-cell x/y halo
-// of (u, v, w, T) are staged in shared memory, x and y derivatives read the
-// tile, z derivatives read the neighbouring planes from global memory
-// (coalesced rows).  T is the array the stage kernel stores (p/(rho Rgas)).
+// A block owns a 32 x 8 column of nodes and marches along z (see the kernel).
+// T is the array the stage kernel stores (p/(rho Rgas)).
 //
 // The divergence of these fluxes (compute_vis_flux, ViscousFlux.cpp:210-255)
 // is added by the three sweeps, each differencing its direction's fluxes
@@ -33,6 +31,7 @@ struct ViscArgs {
     Layout L;
     int periodic[3];
     R h[3];
+    R dinv[3][3];           // per direction: 1/(2h), 1/(12h), 1/(60h)
     R mu0, S, cp_over_pr;
 };
 
@@ -63,57 +62,118 @@ __device__ __forceinline__ R sutherland(R mu0, R S, R T) {
     return mu0 * (T * sqrt(T)) * (R(1) + S) / (T + S);
 }
 
-constexpr int VTX = 32, VTY = 8, VH = NG;
+constexpr int VTX = 32, VTY = 8, VH = NG, VZC = 16;
 
+// First derivative of the window value f(o), o in [-3, 3], with a block-
+// uniform order; the offsets stay compile-time so the window lives in
+// registers.  dinv = 1/(2h), 1/(12h), 1/(60h) (ViscousFlux.cpp:15-29; order
+// -1 is the reference's backward form, which evaluates to -df/dx).
+template <typename R, typename F>
+__device__ __forceinline__ R dwindow(F f, int order, const R *dinv) {
+    switch (order) {
+        case 6: return (f(3) - R(9) * f(2) + R(45) * f(1) - R(45) * f(-1) + R(9) * f(-2) - f(-3)) * dinv[2];
+        case 4: return (-f(2) + R(8) * f(1) - R(8) * f(-1) + f(-2)) * dinv[1];
+        case 2: return (f(1) - f(-1)) * dinv[0];
+        case 1: return (R(-3) * f(0) + R(4) * f(1) - f(2)) * dinv[0];
+        default: return (R(-3) * f(0) + R(4) * f(-1) - f(-2)) * dinv[0];
+    }
+}
+
+template <typename R, typename F>
+__device__ __forceinline__ R dtile(F f, int order, const R *dinv) {
+    if (order == 6)
+        return (f(3) - R(9) * f(2) + R(45) * f(1) - R(45) * f(-1) + R(9) * f(-2) - f(-3)) * dinv[2];
+    if (order == 1 || order == -1) return (R(-3) * f(0) + R(4) * f(order) - f(2 * order)) * dinv[0];
+    if (order == 2) return (f(1) - f(-1)) * dinv[0];
+    return (-f(2) + R(8) * f(1) - R(8) * f(-1) + f(-2)) * dinv[1];
+}
+
+// A block owns a 32 x 8 column of nodes and marches up VZC planes: each
+// thread keeps its node's (u, v, w, T) of planes k-3 .. k+3 in registers and
+// loads one new plane per step; the x/y derivatives read the plane's tile
+// (with its 3-cell halo) from shared memory.  Every input value is read from
+// memory about once per use plane instead of once per neighbour.
 template <typename R>
 __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a) {
-    __shared__ R sm[4][VTY + 2 * VH][VTX + 2 * VH];
+    // two plane tiles: the next plane's tile is copied (cp.async) while the
+    // current one is differenced
+    __shared__ __align__(16) R sm[2][4][VTY + 2 * VH][VTX + 2 * VH];
     const Layout &L = a.L;
-    const int x0 = blockIdx.x * VTX, y0 = blockIdx.y * VTY, k = blockIdx.z + NG;
-    const R *src[4] = {a.W[1], a.W[2], a.W[3], a.T};
-    // tile + halo: ghost-inclusive coordinates (x0 + tx, y0 + ty)
-    for (int t = threadIdx.y * VTX + threadIdx.x; t < (VTX + 2 * VH) * (VTY + 2 * VH); t += VTX * VTY) {
-        const int tx = t % (VTX + 2 * VH), ty = t / (VTX + 2 * VH);
-        const int gx = x0 + tx, gy = y0 + ty;
-        if (gx < L.sx && gy < L.sy) {
-            const long id = L.at(gx, gy, k);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) sm[q][ty][tx] = src[q][id];
-        }
-    }
-    __syncthreads();
+    const int x0 = blockIdx.x * VTX, y0 = blockIdx.y * VTY;
+    const int kb = blockIdx.z * VZC, ke = min(kb + VZC, L.nz);
     const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
-    if (i >= L.nx || j >= L.ny) return;
+    const bool in = i < L.nx && j < L.ny;
+    const R *src[4] = {a.W[1], a.W[2], a.W[3], a.T};
+    const long zs = (long)L.px * L.sy;
+    const long col = L.at(min(i, L.nx - 1) + NG, min(j, L.ny - 1) + NG, 0);  // ghost-inclusive plane 0
     const int ox = visc_order(i, L.nx, a.periodic[0]);
     const int oy = visc_order(j, L.ny, a.periodic[1]);
-    const int oz = visc_order(k - NG, L.nz, a.periodic[2]);
     const int cx = threadIdx.x + VH, cy = threadIdx.y + VH;
-    const long c = L.at(i + NG, j + NG, k);
-    const long zs = (long)L.px * L.sy;
-    R g[4][3];
+    auto fetch_tile = [&](int buf, int k) {  // plane k (interior index), ghost-inclusive x/y
+        for (int t = threadIdx.y * VTX + threadIdx.x; t < (VTX + 2 * VH) * (VTY + 2 * VH); t += VTX * VTY) {
+            const int tx = t % (VTX + 2 * VH), ty = t / (VTX + 2 * VH);
+            const int gx = x0 + tx, gy = y0 + ty;
+            if (gx < L.sx && gy < L.sy) {
+                const long id = L.at(gx, gy, k + NG);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        g[q][0] = dstencil<R>([&](int o) { return sm[q][cy][cx + o]; }, ox, a.h[0]);
-        g[q][1] = dstencil<R>([&](int o) { return sm[q][cy + o][cx]; }, oy, a.h[1]);
-        const R *f = src[q];
-        g[q][2] = dstencil<R>([&](int o) { return f[c + o * zs]; }, oz, a.h[2]);
+                for (int q = 0; q < 4; ++q) cp_async(&sm[buf][q][ty][tx], src[q] + id);
+            }
+        }
+        cp_async_commit();
+    };
+    // window: win[q][m] = value at interior plane k - 3 + m (ghost-inclusive k + m)
+    R win[4][7], nxt[4];
+    fetch_tile(0, kb);
+#pragma unroll
+    for (int m = 0; m < 6; ++m)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) win[q][m] = src[q][col + (long)(kb + m) * zs];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) nxt[q] = src[q][col + (long)(kb + 6) * zs];
+    for (int k = kb; k < ke; ++k) {
+        const int buf = (k - kb) & 1;
+        const bool more = k + 1 < ke;
+        if (more) fetch_tile(buf ^ 1, k + 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) win[q][6] = nxt[q];
+        if (more) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) nxt[q] = src[q][col + (long)(k + 7) * zs];
+        }
+        if (more) cp_async_wait<1>(); else cp_async_wait<0>();  // this plane's tile landed
+        __syncthreads();
+        if (in) {
+            const int oz = visc_order(k, L.nz, a.periodic[2]);
+            R g[4][3];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                g[q][0] = dtile<R>([&](int o) { return sm[buf][q][cy][cx + o]; }, ox, a.dinv[0]);
+                g[q][1] = dtile<R>([&](int o) { return sm[buf][q][cy + o][cx]; }, oy, a.dinv[1]);
+                g[q][2] = dwindow<R>([&](int o) { return win[q][3 + o]; }, oz, a.dinv[2]);
+            }
+            const R T = win[3][3];
+            const R mu = sutherland(a.mu0, a.S, T);
+            const R ux = g[0][0], uy = g[0][1], uz = g[0][2], vx = g[1][0], vy = g[1][1], vz = g[1][2];
+            const R wx = g[2][0], wy = g[2][1], wz = g[2][2], Tx = g[3][0], Ty = g[3][1], Tz = g[3][2];
+            const R div = ux + vy + wz;
+            const R m2 = R(2) * mu, m23 = R(2.0 / 3.0) * mu * div;
+            const R txx = m2 * ux - m23, tyy = m2 * vy - m23, tzz = m2 * wz - m23;
+            const R txy = mu * (uy + vx), txz = mu * (uz + wx), tyz = mu * (vz + wy);
+            const R kq = mu * a.cp_over_pr;
+            const R u = win[0][3], v = win[1][3], w = win[2][3];
+            const long o = ((long)k * L.ny + j) * L.nx + i;
+            a.V[0][o] = txx; a.V[1][o] = tyy; a.V[2][o] = tzz;
+            a.V[3][o] = txy; a.V[4][o] = txz; a.V[5][o] = tyz;
+            a.V[6][o] = u * txx + v * txy + w * txz + kq * Tx;
+            a.V[7][o] = u * txy + v * tyy + w * tyz + kq * Ty;
+            a.V[8][o] = u * txz + v * tyz + w * tzz + kq * Tz;
+        }
+#pragma unroll
+        for (int m = 0; m < 6; ++m)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) win[q][m] = win[q][m + 1];
+        __syncthreads();  // this tile's reads done before it is refilled
     }
-    const R T = sm[3][cy][cx];
-    const R mu = sutherland(a.mu0, a.S, T);
-    const R ux = g[0][0], uy = g[0][1], uz = g[0][2], vx = g[1][0], vy = g[1][1], vz = g[1][2];
-    const R wx = g[2][0], wy = g[2][1], wz = g[2][2], Tx = g[3][0], Ty = g[3][1], Tz = g[3][2];
-    const R div = ux + vy + wz;
-    const R m2 = R(2) * mu, m23 = R(2.0 / 3.0) * mu * div;
-    const R txx = m2 * ux - m23, tyy = m2 * vy - m23, tzz = m2 * wz - m23;
-    const R txy = mu * (uy + vx), txz = mu * (uz + wx), tyz = mu * (vz + wy);
-    const R kq = mu * a.cp_over_pr;
-    const R u = sm[0][cy][cx], v = sm[1][cy][cx], w = sm[2][cy][cx];
-    const long o = ((long)(k - NG) * L.ny + j) * L.nx + i;
-    a.V[0][o] = txx; a.V[1][o] = tyy; a.V[2][o] = tzz;
-    a.V[3][o] = txy; a.V[4][o] = txz; a.V[5][o] = tyz;
-    a.V[6][o] = u * txx + v * txy + w * txz + kq * Tx;
-    a.V[7][o] = u * txy + v * tyy + w * tyz + kq * Ty;
-    a.V[8][o] = u * txz + v * tyz + w * tzz + kq * Tz;
 }
 
 // All 12 derivatives at interior node (i,j,k) (ghost-inclusive indices), for
