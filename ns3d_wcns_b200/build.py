@@ -19,7 +19,11 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libns3d_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
+# -prec-div/-prec-sqrt=false affect single precision only: the FP32 stencil
+# arithmetic of the mixed path (accuracy-bounded, no bitwise contract) uses the
+# fast division and square root; every FP64 operation stays IEEE.
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
+              "-prec-div=false", "-prec-sqrt=false"]
 
 
 def _nvcc() -> str:

@@ -12,6 +12,8 @@
 // stencils -> chain rule through u = m/rho, T = p/(rho Rgas)).
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "adjoint.cuh"
 #include "adjoint_api.cuh"
 #include "common.cuh"
@@ -48,11 +50,20 @@ __device__ __forceinline__ void cons_at(const AdjArgs &a, int i, int j, int k, d
 
 // ---------------------------------------------------------------- inviscid
 
-template <int DIR>
-__global__ void __launch_bounds__(128) adj_face_kernel(AdjArgs a) {
+// One thread per face.  The stencil and the face states are staged in the
+// thread's own shared-memory column, so the per-variable interpolation
+// passes run as rolled loops without local-memory arrays; the Riemann VJP
+// (all five variables coupled) runs in registers in between.
+constexpr int ADJ_T = 128;
+
+template <int DIR, int INTERP, int RS>
+__global__ void __launch_bounds__(ADJ_T) adj_face_kernel(AdjArgs a) {
+    __shared__ double sSt[30][ADJ_T];  // conserved stencil, row q*6 + m
+    __shared__ double sLR[10][ADJ_T];  // UL, UR; then their adjoints
+    const int tid = threadIdx.x;
     const Idx I{a.L.nx, a.L.ny, a.L.nz};
     const long nface = (long)I.nx * I.ny * I.nz;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long t = (long)blockIdx.x * blockDim.x + tid;
     if (t >= nface) return;
     const int i = (int)(t % I.nx), j = (int)((t / I.nx) % I.ny), k = (int)(t / ((long)I.nx * I.ny));
     // face j' + 1/2 along DIR with j' = the cell coordinate along DIR
@@ -62,9 +73,9 @@ __global__ void __launch_bounds__(128) adj_face_kernel(AdjArgs a) {
     for (int q = 0; q < 5; ++q) {
         const double *r = a.Rb[q];
         auto R = [&](int o) { return r[shifted(I, i, j, k, DIR, o)]; };
-        Fb[q] = -ih * (C1 * (R(0) - R(1)) + C3 * (R(-1) - R(2)) + C5 * (R(-2) - R(3)));
+        Fb[q] = -ih * a.rbs * (C1 * (R(0) - R(1)) + C3 * (R(-1) - R(2)) + C5 * (R(-2) - R(3)));
     }
-    double U[5][6];
+#pragma unroll
     for (int m = 0; m < 6; ++m) {
         int ii = i, jj = j, kk = k;
         if (DIR == 0) ii = wrapn(i + m - 2, I.nx);
@@ -73,18 +84,180 @@ __global__ void __launch_bounds__(128) adj_face_kernel(AdjArgs a) {
         double Uc[5];
         cons_at(a, ii, jj, kk, Uc);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) U[q][m] = Uc[q];
+        for (int q = 0; q < 5; ++q) sSt[q * 6 + m][tid] = Uc[q];
     }
-    double Ub[5][6];
+    // forward interpolation, one variable at a time
+#pragma unroll 1
+    for (int q = 0; q < 5; ++q) {
+        double f[6];
 #pragma unroll
-    for (int q = 0; q < 5; ++q)
+        for (int m = 0; m < 6; ++m) f[m] = sSt[q * 6 + m][tid];
+        double l, r;
+        if constexpr (INTERP == 0) {
+            const double fr[5] = {f[5], f[4], f[3], f[2], f[1]};
+            l = adj::weno5_fwd(f);
+            r = adj::weno5_fwd(fr);
+        } else {
+            l = 0.0; r = 0.0;
 #pragma unroll
-        for (int m = 0; m < 6; ++m) Ub[q][m] = 0.0;
-    adj::face_vjp<DIR, double>(a.interp, a.riemann, a.lin, a.gamma, U, Fb, Ub);
+            for (int m = 0; m < 6; ++m) { l += a.lin[m] * f[m]; r += a.lin[m] * f[5 - m]; }
+        }
+        sLR[q][tid] = l;
+        sLR[5 + q][tid] = r;
+    }
+    double UL[5], UR[5], ULb[5] = {0, 0, 0, 0, 0}, URb[5] = {0, 0, 0, 0, 0};
 #pragma unroll
-    for (int m = 0; m < 6; ++m)
+    for (int q = 0; q < 5; ++q) { UL[q] = sLR[q][tid]; UR[q] = sLR[5 + q][tid]; }
+    if constexpr (RS == 0) adj::roe_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
+    else if constexpr (RS == 1) adj::rusanov_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
+    else adj::hll_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
 #pragma unroll
-        for (int q = 0; q < 5; ++q) a.G[m * 5 + q][t] = Ub[q][m];
+    for (int q = 0; q < 5; ++q) { sLR[q][tid] = ULb[q]; sLR[5 + q][tid] = URb[q]; }
+    // interpolation VJP, one variable at a time, straight into the face store
+#pragma unroll 1
+    for (int q = 0; q < 5; ++q) {
+        double f[6], gb[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) f[m] = sSt[q * 6 + m][tid];
+        const double lb = sLR[q][tid], rb = sLR[5 + q][tid];
+        if constexpr (INTERP == 0) {
+            double fbl[5] = {0, 0, 0, 0, 0}, fbr[5] = {0, 0, 0, 0, 0};
+            adj::weno5_vjp(f, lb, fbl);
+            const double fr[5] = {f[5], f[4], f[3], f[2], f[1]};
+            adj::weno5_vjp(fr, rb, fbr);
+            gb[0] = fbl[0]; gb[5] = fbr[0];
+#pragma unroll
+            for (int m = 1; m < 5; ++m) gb[m] = fbl[m] + fbr[5 - m];
+        } else {
+#pragma unroll
+            for (int m = 0; m < 6; ++m) gb[m] = a.lin[m] * lb + a.lin[5 - m] * rb;
+        }
+#pragma unroll
+        for (int m = 0; m < 6; ++m) a.G[m * 5 + q][t] = gb[m];
+    }
+}
+
+// Whole periodic lines in one block (line length n <= 256): the block
+// converts its cells once, computes the face VJPs of the line (same
+// arithmetic as adj_face_kernel) into shared memory and gathers them, in
+// the same order as adj_face_gather_kernel, so the per-face store never
+// reaches global memory.  lpb lines per block; threads = lpb * n.
+template <int DIR, int INTERP, int RS>
+__global__ void __launch_bounds__(256) adj_line_kernel(AdjArgs a, int lpb, int first) {
+    extern __shared__ __align__(16) double smem_adj[];
+    const Idx I{a.L.nx, a.L.ny, a.L.nz};
+    const int n = DIR == 0 ? I.nx : (DIR == 1 ? I.ny : I.nz);
+    const int T = lpb * n;
+    double *sU = smem_adj, *sR = sU + 5 * T, *sG = sR + 5 * T, *sLR = sG + 30 * T;
+    const int l = DIR == 0 ? threadIdx.y : threadIdx.x;
+    const int c = DIR == 0 ? threadIdx.x : threadIdx.y;
+    // [line][pos] along x, [pos][line] across lines: warps read contiguous words
+    auto sidx = [&](int cc) { return DIR == 0 ? l * n + cc : cc * lpb + l; };
+    auto at = [&](int cc) { return sidx(wrapn(cc, n)); };
+    const int tid = sidx(c);
+    const long nlines = DIR == 0 ? (long)I.ny * I.nz : (DIR == 1 ? (long)I.nx * I.nz : (long)I.nx * I.ny);
+    const long g = (long)blockIdx.x * lpb + l;
+    const bool ok = g < nlines;
+    int i, j, k;
+    if (DIR == 0) { i = c; j = (int)(g % I.ny); k = (int)(g / I.ny); }
+    else if (DIR == 1) { i = (int)(g % I.nx); j = c; k = (int)(g / I.nx); }
+    else { i = (int)(g % I.nx); j = (int)(g / I.nx); k = c; }
+    const long tc = ok ? I.at(i, j, k) : 0;
+    if (ok) {
+        double Uc[5];
+        cons_at(a, i, j, k, Uc);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) { sU[q * T + tid] = Uc[q]; sR[q * T + tid] = a.rbs * a.Rb[q][tc]; }
+    }
+    __syncthreads();
+    if (ok) {
+        // face c + 1/2
+        const double ih = a.inv_h[DIR];
+        double Fb[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            auto R = [&](int o) { return sR[q * T + at(c + o)]; };
+            Fb[q] = -ih * (C1 * (R(0) - R(1)) + C3 * (R(-1) - R(2)) + C5 * (R(-2) - R(3)));
+        }
+#pragma unroll 1
+        for (int q = 0; q < 5; ++q) {
+            double f[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) f[m] = sU[q * T + at(c - 2 + m)];
+            double lv, rv;
+            if constexpr (INTERP == 0) {
+                const double fr[5] = {f[5], f[4], f[3], f[2], f[1]};
+                lv = adj::weno5_fwd(f);
+                rv = adj::weno5_fwd(fr);
+            } else {
+                lv = 0.0; rv = 0.0;
+#pragma unroll
+                for (int m = 0; m < 6; ++m) { lv += a.lin[m] * f[m]; rv += a.lin[m] * f[5 - m]; }
+            }
+            sLR[q * T + tid] = lv;
+            sLR[(5 + q) * T + tid] = rv;
+        }
+        double UL[5], UR[5], ULb[5] = {0, 0, 0, 0, 0}, URb[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < 5; ++q) { UL[q] = sLR[q * T + tid]; UR[q] = sLR[(5 + q) * T + tid]; }
+        if constexpr (RS == 0) adj::roe_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
+        else if constexpr (RS == 1) adj::rusanov_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
+        else adj::hll_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) { sLR[q * T + tid] = ULb[q]; sLR[(5 + q) * T + tid] = URb[q]; }
+#pragma unroll 1
+        for (int q = 0; q < 5; ++q) {
+            double f[6], gb[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) f[m] = sU[q * T + at(c - 2 + m)];
+            const double lb = sLR[q * T + tid], rb = sLR[(5 + q) * T + tid];
+            if constexpr (INTERP == 0) {
+                double fbl[5] = {0, 0, 0, 0, 0}, fbr[5] = {0, 0, 0, 0, 0};
+                adj::weno5_vjp(f, lb, fbl);
+                const double fr[5] = {f[5], f[4], f[3], f[2], f[1]};
+                adj::weno5_vjp(fr, rb, fbr);
+                gb[0] = fbl[0]; gb[5] = fbr[0];
+#pragma unroll
+                for (int m = 1; m < 5; ++m) gb[m] = fbl[m] + fbr[5 - m];
+            } else {
+#pragma unroll
+                for (int m = 0; m < 6; ++m) gb[m] = a.lin[m] * lb + a.lin[5 - m] * rb;
+            }
+#pragma unroll
+            for (int m = 0; m < 6; ++m) sG[(m * 5 + q) * T + tid] = gb[m];
+        }
+    }
+    __syncthreads();
+    if (ok) {
+        // cell c gathers the m-th contribution of face c - m + 2
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            double s = first ? 0.0 : a.Ub[q][tc];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) s += sG[(m * 5 + q) * T + at(c + 2 - m)];
+            a.Ub[q][tc] = s;
+        }
+    }
+}
+
+template <int DIR, int INTERP, int RS>
+cudaError_t launch_line(const AdjArgs &a, int first, cudaStream_t st) {
+    const int n = DIR == 0 ? a.L.nx : (DIR == 1 ? a.L.ny : a.L.nz);
+    const int lpb = n <= 128 ? 128 / n : 1;
+    const long nlines = DIR == 0 ? (long)a.L.ny * a.L.nz : (DIR == 1 ? (long)a.L.nx * a.L.nz : (long)a.L.nx * a.L.ny);
+    const size_t smem = (size_t)50 * lpb * n * sizeof(double);
+    static unsigned configured = 0;  // one bit per device ordinal
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured & (1u << (dev & 31)))) {
+        cudaError_t e = cudaFuncSetAttribute(adj_line_kernel<DIR, INTERP, RS>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, 50 * 256 * 8);
+        if (e != cudaSuccess) return e;
+        configured |= 1u << (dev & 31);
+    }
+    dim3 block(DIR == 0 ? n : lpb, DIR == 0 ? lpb : n);
+    adj_line_kernel<DIR, INTERP, RS><<<(unsigned)((nlines + lpb - 1) / lpb), block, smem, st>>>(a, lpb, first);
+    return cudaGetLastError();
 }
 
 // cell c gathers m-th stencil contributions of faces c - m + 2
@@ -124,7 +297,7 @@ __global__ void __launch_bounds__(128) adj_visc_node_kernel(AdjArgs a) {
         double s = 0.0;
 #pragma unroll
         for (int o = -3; o <= 3; ++o) s += D6[o + 3] * r[shifted(I, i, j, k, d, -o)];
-        return s * a.inv_h[d];
+        return s * (a.inv_h[d] * a.rbs);
     };
     double Vb[9];
     Vb[0] = DT(a.Rb[1], 0);                    // txx: x-term of rhou
@@ -234,18 +407,74 @@ __global__ void velocity_grad_kernel(AdjArgs a, const double *const *Ub, double 
 
 int blocks_for(long n, int t) { return (int)((n + t - 1) / t); }
 
+// tab[5*slot + q]: slot 0 UB (adjoint of the step's result / of its input),
+// 1 ACC, 2 SB, 3 RB
+__global__ void step_combine_kernel(int which, double *const *tab, double dt, long n) {
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            double *UB = tab[q], *ACC = tab[5 + q], *SB = tab[10 + q], *RB = tab[15 + q];
+            if (which == 1) {
+                const double u = UB[t];
+                ACC[t] = u * (1.0 / 3.0);
+                SB[t] = u * (2.0 / 3.0);
+            } else if (which == 2) {
+                const double sb = SB[t], s4 = 0.25 * sb;
+                ACC[t] += 0.75 * sb;
+                SB[t] = s4;
+                RB[t] = dt * s4;
+            } else {
+                UB[t] = ACC[t] + SB[t];
+            }
+        }
+}
+
 }  // namespace
 
 cudaError_t adj_rhs_vjp(const AdjArgs &a, cudaStream_t st, long *launches) {
     const long n = (long)a.L.nx * a.L.ny * a.L.nz;
     const int nb = blocks_for(n, 128);
-    adj_face_kernel<0><<<nb, 128, 0, st>>>(a);
-    adj_face_gather_kernel<0><<<nb, 128, 0, st>>>(a, a.first);
-    adj_face_kernel<1><<<nb, 128, 0, st>>>(a);
-    adj_face_gather_kernel<1><<<nb, 128, 0, st>>>(a, 0);
-    adj_face_kernel<2><<<nb, 128, 0, st>>>(a);
-    adj_face_gather_kernel<2><<<nb, 128, 0, st>>>(a, 0);
-    *launches += 6;
+    // riemann codes here: 0 Roe, 1 Rusanov, 3 HLL (face_vjp_t takes 2 for HLL)
+    const int rs = a.riemann == 3 ? 2 : a.riemann;
+    auto face = [&](auto dir_tag) {
+        constexpr int D = decltype(dir_tag)::value;
+        if (a.interp == 0) {
+            if (rs == 0) adj_face_kernel<D, 0, 0><<<nb, 128, 0, st>>>(a);
+            else if (rs == 1) adj_face_kernel<D, 0, 1><<<nb, 128, 0, st>>>(a);
+            else adj_face_kernel<D, 0, 2><<<nb, 128, 0, st>>>(a);
+        } else {
+            if (rs == 0) adj_face_kernel<D, 2, 0><<<nb, 128, 0, st>>>(a);
+            else if (rs == 1) adj_face_kernel<D, 2, 1><<<nb, 128, 0, st>>>(a);
+            else adj_face_kernel<D, 2, 2><<<nb, 128, 0, st>>>(a);
+        }
+    };
+    auto line = [&](auto dir_tag, int first) -> cudaError_t {
+        constexpr int D = decltype(dir_tag)::value;
+        if (a.interp == 0) {
+            if (rs == 0) return launch_line<D, 0, 0>(a, first, st);
+            if (rs == 1) return launch_line<D, 0, 1>(a, first, st);
+            return launch_line<D, 0, 2>(a, first, st);
+        }
+        if (rs == 0) return launch_line<D, 2, 0>(a, first, st);
+        if (rs == 1) return launch_line<D, 2, 1>(a, first, st);
+        return launch_line<D, 2, 2>(a, first, st);
+    };
+    const bool fused = a.L.nx <= 256 && a.L.ny <= 256 && a.L.nz <= 256;
+    if (fused) {
+        cudaError_t e;
+        if ((e = line(std::integral_constant<int, 0>{}, a.first)) != cudaSuccess) return e;
+        if ((e = line(std::integral_constant<int, 1>{}, 0)) != cudaSuccess) return e;
+        if ((e = line(std::integral_constant<int, 2>{}, 0)) != cudaSuccess) return e;
+        *launches += 3;
+    } else {
+        face(std::integral_constant<int, 0>{});
+        adj_face_gather_kernel<0><<<nb, 128, 0, st>>>(a, a.first);
+        face(std::integral_constant<int, 1>{});
+        adj_face_gather_kernel<1><<<nb, 128, 0, st>>>(a, 0);
+        face(std::integral_constant<int, 2>{});
+        adj_face_gather_kernel<2><<<nb, 128, 0, st>>>(a, 0);
+        *launches += 6;
+    }
     if (a.mu0 != 0.0) {
         adj_visc_node_kernel<<<nb, 128, 0, st>>>(a);
         adj_visc_gather_kernel<<<nb, 128, 0, st>>>(a);
@@ -256,6 +485,11 @@ cudaError_t adj_rhs_vjp(const AdjArgs &a, cudaStream_t st, long *launches) {
 
 cudaError_t adj_axpby(double *const *y, const double *const *x, double alpha, double beta, long n, cudaStream_t st) {
     axpby_kernel<<<blocks_for(n, 256) < 4096 ? blocks_for(n, 256) : 4096, 256, 0, st>>>(y, x, alpha, beta, n);
+    return cudaGetLastError();
+}
+
+cudaError_t adj_step_combine(int which, double *const *tab, double dt, long n, cudaStream_t st) {
+    step_combine_kernel<<<blocks_for(n, 256) < 4096 ? blocks_for(n, 256) : 4096, 256, 0, st>>>(which, tab, dt, n);
     return cudaGetLastError();
 }
 

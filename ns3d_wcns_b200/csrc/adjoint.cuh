@@ -159,6 +159,7 @@ NS3D_HD void roe_vjp(const R *UL, const R *UR, R g, const R *Fb, R *ULb, R *URb)
     R V = DIR == 0 ? ub : (DIR == 1 ? vb : wb);
     R phi = R(0.5) * gm1 * q2b;
     R dU[5];
+#pragma unroll
     for (int n = 0; n < 5; ++n) dU[n] = UR[n] - UL[n];
     const R dUn = dU[1 + DIR];
     R t = phi * dU[0] + gm1 * (dU[4] - ub * dU[1] - vb * dU[2] - wb * dU[3]);
@@ -172,11 +173,14 @@ NS3D_HD void roe_vjp(const R *UL, const R *UR, R g, const R *Fb, R *ULb, R *URb)
     const R e0 = DIR == 0 ? R(1) : R(0), e1 = DIR == 1 ? R(1) : R(0), e2 = DIR == 2 ? R(1) : R(0);
     // ---- reverse
     R Db[5];
+#pragma unroll
     for (int n = 0; n < 5; ++n) Db[n] = R(-0.5) * Fb[n];
     R FLb[5], FRb[5];
+#pragma unroll
     for (int n = 0; n < 5; ++n) { FLb[n] = R(0.5) * Fb[n]; FRb[n] = R(0.5) * Fb[n]; }
     R dUb[5];
     R lvfb = R(0);
+#pragma unroll
     for (int n = 0; n < 5; ++n) { lvfb += Db[n] * dU[n]; dUb[n] = lvf * Db[n]; }
     R k0b = Db[0] + Db[1] * (ub - c * e0) + Db[2] * (vb - c * e1) + Db[3] * (wb - c * e2) + Db[4] * (Hb - c * V);
     R k4b = Db[0] + Db[1] * (ub + c * e0) + Db[2] * (vb + c * e1) + Db[3] * (wb + c * e2) + Db[4] * (Hb + c * V);
@@ -244,6 +248,7 @@ NS3D_HD void roe_vjp(const R *UL, const R *UR, R g, const R *Fb, R *ULb, R *URb)
     pflux_vjp<DIR, R>(Rs, FRb, uRb, vRb, wRb, pRb, ERb, rRb);
     side_vjp(L, g, uLb, vLb, wLb, pLb, ELb, rLb, ULb);
     side_vjp(Rs, g, uRb, vRb, wRb, pRb, ERb, rRb, URb);
+#pragma unroll
     for (int n = 0; n < 5; ++n) { URb[n] += dUb[n]; ULb[n] -= dUb[n]; }
 }
 
@@ -257,6 +262,7 @@ NS3D_HD void rusanov_vjp(const R *UL, const R *UR, R g, const R *Fb, R *ULb, R *
     bool left = !(sl < sr);  // std::max(a,b) returns a unless a < b
     R smax = left ? sl : sr;
     R FLb[5], FRb[5], smaxb = R(0);
+#pragma unroll
     for (int n = 0; n < 5; ++n) {
         FLb[n] = R(0.5) * Fb[n]; FRb[n] = R(0.5) * Fb[n];
         smaxb += R(-0.5) * Fb[n] * (UR[n] - UL[n]);
@@ -304,12 +310,15 @@ NS3D_HD void hll_vjp(const R *UL, const R *UR, R g, const R *Fb, R *ULb, R *URb)
     R uLb = 0, vLb = 0, wLb = 0, pLb = 0, ELb = 0, rLb = 0, uRb = 0, vRb = 0, wRb = 0, pRb = 0, ERb = 0, rRb = 0;
     R FLb[5] = {0, 0, 0, 0, 0}, FRb[5] = {0, 0, 0, 0, 0};
     if (SL >= R(0)) {
+#pragma unroll
         for (int n = 0; n < 5; ++n) FLb[n] = Fb[n];
     } else if (SR <= R(0)) {
+#pragma unroll
         for (int n = 0; n < 5; ++n) FRb[n] = Fb[n];
     } else {
         R id = R(1) / (SR - SL);
         R SLb = 0, SRb = 0;
+#pragma unroll
         for (int n = 0; n < 5; ++n) {
             R dUn = UR[n] - UL[n];
             R F = (SR * FL[n] - SL * FR[n] + SL * SR * dUn) * id;
@@ -350,15 +359,18 @@ NS3D_HD void hll_vjp(const R *UL, const R *UR, R g, const R *Fb, R *ULb, R *URb)
 // Component-wise WCNS face flux (WCNS_Riemann_InviscidFlux, InviscousFlux.cpp:
 // 146-268 with char_recon = false): U[n][m], m = cells i-2..i+3.
 // interp: 0 WENO5, 2 MDCD_LINEAR (lin = its six coefficients).
-template <int DIR, typename R>
-NS3D_HD void face_vjp(int interp, int riemann, const R *lin, R g, const R U[5][6], const R *Fb, R Ub[5][6]) {
+template <int DIR, typename R, int INTERP, int RS>
+NS3D_HD void face_vjp_t(const R *lin, R g, const R U[5][6], const R *Fb, R Ub[5][6]) {
+    constexpr int interp = INTERP, riemann = RS;
     R UL[5], UR[5];
+#pragma unroll
     for (int n = 0; n < 5; ++n) {
         const R *f = U[n];
         R fr[6] = {f[5], f[4], f[3], f[2], f[1], f[0]};
         if (interp == 0) { UL[n] = weno5_fwd(f); UR[n] = weno5_fwd(fr); }
         else {
             R a = R(0), b = R(0);
+#pragma unroll
             for (int m = 0; m < 6; ++m) { a += lin[m] * f[m]; b += lin[m] * fr[m]; }
             UL[n] = a; UR[n] = b;
         }
@@ -367,19 +379,37 @@ NS3D_HD void face_vjp(int interp, int riemann, const R *lin, R g, const R U[5][6
     if (riemann == 0) roe_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
     else if (riemann == 1) rusanov_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
     else hll_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
+#pragma unroll
     for (int n = 0; n < 5; ++n) {
         const R *f = U[n];
         if (interp == 0) {
             R fbl[5] = {0, 0, 0, 0, 0};
             weno5_vjp(f, ULb[n], fbl);
+#pragma unroll
             for (int m = 0; m < 5; ++m) Ub[n][m] += fbl[m];
             R fr[5] = {f[5], f[4], f[3], f[2], f[1]};
             R fbr[5] = {0, 0, 0, 0, 0};
             weno5_vjp(fr, URb[n], fbr);
+#pragma unroll
             for (int m = 0; m < 5; ++m) Ub[n][5 - m] += fbr[m];
         } else {
+#pragma unroll
             for (int m = 0; m < 6; ++m) Ub[n][m] += lin[m] * ULb[n] + lin[5 - m] * URb[n];
         }
+    }
+}
+
+// run-time selection (interp 0 WENO5 / 2 MDCD_LINEAR; riemann 0 Roe, 1 Rusanov, 2 HLL)
+template <int DIR, typename R>
+NS3D_HD void face_vjp(int interp, int riemann, const R *lin, R g, const R U[5][6], const R *Fb, R Ub[5][6]) {
+    if (interp == 0) {
+        if (riemann == 0) face_vjp_t<DIR, R, 0, 0>(lin, g, U, Fb, Ub);
+        else if (riemann == 1) face_vjp_t<DIR, R, 0, 1>(lin, g, U, Fb, Ub);
+        else face_vjp_t<DIR, R, 0, 2>(lin, g, U, Fb, Ub);
+    } else {
+        if (riemann == 0) face_vjp_t<DIR, R, 2, 0>(lin, g, U, Fb, Ub);
+        else if (riemann == 1) face_vjp_t<DIR, R, 2, 1>(lin, g, U, Fb, Ub);
+        else face_vjp_t<DIR, R, 2, 2>(lin, g, U, Fb, Ub);
     }
 }
 

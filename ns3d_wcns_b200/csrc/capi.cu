@@ -506,12 +506,14 @@ AdjArgs adj_args(ns3d_handle *h, double *const W[5], const double *const Rb[5], 
     a.interp = h->P.interpolation; a.riemann = h->P.riemann_solver == NS3D_HLL ? 3 : h->P.riemann_solver;
     for (int m = 0; m < 6; ++m) a.lin[m] = h->sp64.lin[m];
     a.first = 0;
+    a.rbs = 1.0;
     return a;
 }
 
-// Ub_target += (dR/dU at W)^T Rb
-int vjp_rhs_async(ns3d_handle *h, double *const W[5], int rb_slot, int target_slot) {
+// Ub_target += (dR/dU at W)^T (rbs * Rb)
+int vjp_rhs_async(ns3d_handle *h, double *const W[5], int rb_slot, int target_slot, double rbs = 1.0) {
     AdjArgs a = adj_args(h, W, h->ab[rb_slot], h->ab[target_slot]);
+    a.rbs = rbs;
     cudaError_t e = adj_rhs_vjp(a, h->stream, &h->launches);
     if (e != cudaSuccess) return cuda_fail(h, e, "adjoint kernels");
     return NS3D_OK;
@@ -528,23 +530,26 @@ int axpby_slot(ns3d_handle *h, int y, int x, double alpha, double beta) {
 
 // Backward through one RK3 step whose stage states are W0, W1, W2.
 // Slot 0 holds the adjoint of the step's result on entry and of its input on
-// exit; slots 1 (accumulator), 2 (stage adjoint), 3 (rhs adjoint) are scratch.
+// exit; slots 1 (accumulator ACC), 2 (stage adjoint SB), 3 (RHS adjoint RB)
+// are scratch.
 //   U1 = U0 + dt R(U0); U2 = 3/4 U0 + 1/4 (U1 + dt R(U1)); U3 = 1/3 U0 + 2/3 (U2 + dt R(U2))
+// The scalings of the RHS adjoints ride on the VJP kernels' input scale, so
+// one step costs three fused combinations and three RHS VJPs.
 int vjp_step_async(ns3d_handle *h, double *const W0[5], double *const W1[5], double *const W2[5], double dt) {
     int r;
     enum { UB = 0, ACC = 1, SB = 2, RB = 3 };
-    if ((r = axpby_slot(h, RB, UB, (2.0 / 3.0) * dt, 0.0))) return r;
-    if ((r = axpby_slot(h, ACC, UB, 1.0 / 3.0, 0.0))) return r;
-    if ((r = axpby_slot(h, SB, UB, 2.0 / 3.0, 0.0))) return r;
-    if ((r = vjp_rhs_async(h, W2, RB, SB))) return r;          // SB = adjoint of U2
-    if ((r = axpby_slot(h, RB, SB, 0.25 * dt, 0.0))) return r;
-    if ((r = axpby_slot(h, ACC, SB, 0.75, 1.0))) return r;
-    if ((r = axpby_slot(h, SB, SB, 0.0, 0.25))) return r;
-    if ((r = vjp_rhs_async(h, W1, RB, SB))) return r;          // SB = adjoint of U1
-    if ((r = axpby_slot(h, RB, SB, dt, 0.0))) return r;
-    if ((r = axpby_slot(h, ACC, SB, 1.0, 1.0))) return r;
-    if ((r = vjp_rhs_async(h, W0, RB, ACC))) return r;         // ACC = adjoint of U0
-    return axpby_slot(h, UB, ACC, 1.0, 0.0);
+    const long n = (long)h->L64.nx * h->L64.ny * h->L64.nz;
+    auto combine = [&](int which) -> int {
+        cudaError_t e = adj_step_combine(which, h->adj_tab, dt, n, h->stream);
+        h->launches += 1;
+        return e == cudaSuccess ? NS3D_OK : cuda_fail(h, e, "adjoint combination");
+    };
+    if ((r = combine(1))) return r;                                    // ACC = UB/3, SB = 2 UB/3
+    if ((r = vjp_rhs_async(h, W2, UB, SB, (2.0 / 3.0) * dt))) return r;  // SB = adjoint of U2
+    if ((r = combine(2))) return r;                                    // ACC += 3/4 SB, SB /= 4, RB = dt SB
+    if ((r = vjp_rhs_async(h, W1, RB, SB))) return r;                  // SB = adjoint of U1
+    if ((r = combine(3))) return r;                                    // UB = ACC + SB
+    return vjp_rhs_async(h, W0, SB, UB, dt);                           // UB = adjoint of U0
 }
 
 // One forward step that also stores its three stage states.
@@ -1213,7 +1218,18 @@ int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int check
             for (int q = 0; q < 5; ++q)
                 if (cudaMemcpyAsync(ck(n / ce, q), h->S[h->s0][q], bytes, cudaMemcpyDeviceToDevice, h->stream))
                     r = fail(h, NS3D_ERR_CUDA, "checkpoint copy");
-        if (!r) r = rk3_async(h, dt);
+        if (r) break;
+        const int n0_last = (nck - 1) * ce;
+        if (n >= n0_last) {
+            // the last segment keeps its stage states from this pass: the
+            // backward sweep starts there without recomputing it
+            double *st[3][5];
+            for (int b = 0; b < 3; ++b)
+                for (int q = 0; q < 5; ++q) st[b][q] = seg(n - n0_last, b, q);
+            r = rk3_async_store(h, dt, st);
+        } else {
+            r = rk3_async(h, dt);
+        }
     }
     cudaEventRecord(e1, h->stream);
     long recomputed = 0;
@@ -1232,10 +1248,13 @@ int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int check
     // ---- backward: per segment recompute the stage states, then step back
     for (int c = nck - 1; c >= 0 && !r; --c) {
         const int n0 = c * ce, n1 = (n0 + ce < nsteps) ? n0 + ce : nsteps;
-        for (int q = 0; q < 5; ++q)
-            cudaMemcpyAsync(h->S[h->s0][q], ck(c, q), bytes, cudaMemcpyDeviceToDevice, h->stream);
-        r = refresh_T(h);
-        for (int n = n0; n < n1 && !r; ++n) {
+        const bool stored = c == nck - 1;  // stage states kept by the forward pass
+        if (!stored) {
+            for (int q = 0; q < 5; ++q)
+                cudaMemcpyAsync(h->S[h->s0][q], ck(c, q), bytes, cudaMemcpyDeviceToDevice, h->stream);
+            r = refresh_T(h);
+        }
+        for (int n = n0; n < n1 && !r && !stored; ++n) {
             double *st[3][5];
             for (int b = 0; b < 3; ++b)
                 for (int q = 0; q < 5; ++q) st[b][q] = seg(n - n0, b, q);
