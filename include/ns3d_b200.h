@@ -41,9 +41,12 @@ extern "C" {
 #define NS3D_ERR_SIZE (-10)         /* grid larger than an entry point's stated maximum */
 
 /* ------------------------------------------------------------ enumerations */
-/* Same numbering as the reference enums (field_structures.h:131-165). */
+/* Same numbering as the reference enums (field_structures.h:131-165).
+ * NS3D_STEGER_WARMING is this library's addition: the reference declares the
+ * splitting (field_structures.h:113-119) without implementing it. */
 enum { NS3D_WENO5 = 0, NS3D_ZERO = 1, NS3D_MDCD_LINEAR = 2, NS3D_MDCD_HYBRID = 3 };
-enum { NS3D_ROE = 0, NS3D_RUSANOV = 1, NS3D_HLLC = 2, NS3D_HLL = 3, NS3D_HLLC_P = 4, NS3D_AUSM = 5 };
+enum { NS3D_ROE = 0, NS3D_RUSANOV = 1, NS3D_HLLC = 2, NS3D_HLL = 3, NS3D_HLLC_P = 4, NS3D_AUSM = 5,
+       NS3D_STEGER_WARMING = 6 };
 enum { NS3D_PERIODIC = 0, NS3D_WALL = 1, NS3D_SYMMETRY = 2, NS3D_OUTFLOW = 3, NS3D_INFLOW = 4 };
 enum { NS3D_FP64 = 0, NS3D_MIXED = 1 };
 
@@ -63,7 +66,7 @@ typedef struct ns3d_params {
     double mdcd_diss, mdcd_disp;
     double sutherland_s;            /* S/T_ref; reference value 110.4/288.15 */
     int interpolation;              /* NS3D_WENO5 | NS3D_MDCD_LINEAR | NS3D_MDCD_HYBRID */
-    int riemann_solver;             /* NS3D_ROE ... NS3D_AUSM */
+    int riemann_solver;             /* NS3D_ROE ... NS3D_AUSM, NS3D_STEGER_WARMING */
     int char_recon;                 /* 0 component-wise, 1 characteristic-wise */
     int bc[6];                      /* xmin xmax ymin ymax zmin zmax */
     int precision;                  /* NS3D_FP64 (reference parity) | NS3D_MIXED */
@@ -243,6 +246,12 @@ int ns3d_debug_face_vjp(int direction, int interpolation, int riemann, double ga
                         const double *U30, const double *Fbar5, double *out30, double *flux5);
 int ns3d_debug_visc_vjp(double mu0, double S, double cp_over_pr, const double *x4, const double *g12,
                         const double *Vbar9, double *xb4, double *gb12, double *V9);
+/* Host evaluation of the production face flux F(UL, UR) of one Riemann solver
+ * (NS3D_ROE ... NS3D_STEGER_WARMING) along direction 0/1/2, FP64.  Replaces no
+ * reference entry point (the reference's solvers are the static functions of
+ * InviscousFlux.cpp:270-846); for unit tests of the flux functions. */
+int ns3d_debug_riemann(int direction, int riemann, double gamma, const double UL[5], const double UR[5],
+                       double F[5]);
 
 /* ---------------------------------------- scratch-free CFL time step
  * No counterpart in the reference.  For host codes that cannot let a library

@@ -29,13 +29,16 @@ class Interpolation(enum.IntEnum):
 
 
 class RiemannSolver(enum.IntEnum):
-    """Order as field_structures.h:137-144."""
+    """Order as field_structures.h:137-144; StegerWarming is this build's
+    addition (the reference declares the splitting, field_structures.h:113-119,
+    but implements no formula)."""
     Roe = 0
     Rusanov = 1
     HLLC = 2
     HLL = 3
     HLLC_p = 4
     AUSM = 5
+    StegerWarming = 6
 
 
 class BCType(enum.IntEnum):
@@ -208,7 +211,9 @@ def parse_solver_params(text: str) -> Tuple[SolverParams, GridDesc, CartDecomp]:
         elif k == "riemann_solver":
             P.riemann_solver = {"roe": RiemannSolver.Roe, "rusanov": RiemannSolver.Rusanov,
                                 "hllc": RiemannSolver.HLLC, "hll": RiemannSolver.HLL,
-                                "hllc_p": RiemannSolver.HLLC_p, "ausm": RiemannSolver.AUSM}.get(v, P.riemann_solver)
+                                "hllc_p": RiemannSolver.HLLC_p, "ausm": RiemannSolver.AUSM,
+                                "steger_warming": RiemannSolver.StegerWarming,
+                                "stegerwarming": RiemannSolver.StegerWarming}.get(v, P.riemann_solver)
         elif k == "mdcd_diss": P.mdcd_diss = _stod(val)
         elif k == "mdcd_disp": P.mdcd_disp = _stod(val)
         elif k == "global_nx": G.global_nx = _stoi(val)

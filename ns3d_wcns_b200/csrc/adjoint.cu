@@ -509,6 +509,13 @@ cudaError_t adj_velocity_grad(const AdjArgs &a, const double *const *Ub, double 
 
 // ------------------------------------------------- host evaluation for tests
 
+namespace ns3d {
+template <int DIR>
+void riemann_flux_host(const SchemeParams<double> &sp, const double *UL, const double *UR, double *F) {
+    riemann<DIR, double, RUNTIME>(sp, UL, UR, F);
+}
+}  // namespace ns3d
+
 extern "C" int ns3d_debug_face_vjp(int direction, int interpolation, int riemann, double gamma,
                                    const double lin[6], const double *U30, const double *Fbar5, double *out30,
                                    double *flux5) {
@@ -552,5 +559,20 @@ extern "C" int ns3d_debug_visc_vjp(double mu0, double S, double cpr, const doubl
     for (int q = 0; q < 4; ++q)
         for (int d = 0; d < 3; ++d) gb12[3 * q + d] = gb[q][d];
     if (V9) adj::visc_flux_all<double>(mu0, S, cpr, x4, g, V9);
+    return 0;
+}
+
+extern "C" int ns3d_debug_riemann(int direction, int riemann, double gamma, const double UL[5], const double UR[5],
+                                  double F[5]) {
+    using namespace ns3d;
+    if (!UL || !UR || !F || direction < 0 || direction > 2 || riemann < 0 || riemann > 6) return -1;
+    SchemeParams<double> sp;
+    sp.gamma = gamma;
+    for (int m = 0; m < 6; ++m) sp.lin[m] = 0.0;
+    for (int m = 0; m < 4; ++m) sp.hd[m] = 0.0;
+    sp.interp = 0; sp.riemann = riemann; sp.char_recon = 0;
+    if (direction == 0) riemann_flux_host<0>(sp, UL, UR, F);
+    else if (direction == 1) riemann_flux_host<1>(sp, UL, UR, F);
+    else riemann_flux_host<2>(sp, UL, UR, F);
     return 0;
 }

@@ -374,7 +374,7 @@ int ns3d_batch_create(const ns3d_params *params, int n_inst, const ns3d_grid *gr
     *out = nullptr;
     if (params->precision != NS3D_FP64 || params->char_recon) return NS3D_ERR_CONFIG;
     if (params->interpolation == NS3D_ZERO || params->interpolation < 0 || params->interpolation > 3) return NS3D_ERR_CONFIG;
-    if (params->riemann_solver < 0 || params->riemann_solver > 5) return NS3D_ERR_CONFIG;
+    if (params->riemann_solver < 0 || params->riemann_solver > 6) return NS3D_ERR_CONFIG;
     if (!std::isinf(params->Re)) return NS3D_ERR_CONFIG;  // batched problems are inviscid (Re = inf)
     // y and z must be periodic (the quasi-1D cross-section); x takes any boundary type
     for (int f = 2; f < 6; ++f)

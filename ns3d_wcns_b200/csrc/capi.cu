@@ -616,7 +616,7 @@ bool valid_params(const ns3d_params *p, const ns3d_grid *g, std::string &why) {
     if (p->interpolation != NS3D_WENO5 && p->interpolation != NS3D_MDCD_LINEAR && p->interpolation != NS3D_MDCD_HYBRID) {
         why = "unknown interpolation"; return false;
     }
-    if (p->riemann_solver < 0 || p->riemann_solver > 5) { why = "unknown Riemann solver"; return false; }
+    if (p->riemann_solver < 0 || p->riemann_solver > 6) { why = "unknown Riemann solver"; return false; }
     for (int f = 0; f < 6; ++f)
         if (p->bc[f] < 0 || p->bc[f] > 4) { why = "unknown boundary type"; return false; }
     if (p->precision != NS3D_FP64 && p->precision != NS3D_MIXED) { why = "unknown precision"; return false; }

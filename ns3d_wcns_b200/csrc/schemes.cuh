@@ -18,7 +18,7 @@
 namespace ns3d {
 
 enum { I_WENO5 = 0, I_ZERO = 1, I_MDCD_LINEAR = 2, I_MDCD_HYBRID = 3 };
-enum { R_ROE = 0, R_RUSANOV = 1, R_HLLC = 2, R_HLL = 3, R_HLLC_P = 4, R_AUSM = 5 };
+enum { R_ROE = 0, R_RUSANOV = 1, R_HLLC = 2, R_HLL = 3, R_HLLC_P = 4, R_AUSM = 5, R_STEGER_WARMING = 6 };
 constexpr int RUNTIME = -1;
 
 template <typename R>
@@ -402,6 +402,47 @@ NS3D_HD void ausm_flux(const R *UL, const R *UR, R g, R *F) {
     F[4] = md * Hf;
 }
 
+// Steger-Warming flux-vector splitting (J. L. Steger, R. F. Warming, J.
+// Comput. Phys. 40 (1981) 263-293) as a face flux: F = F+(U_L) + F-(U_R).
+// With the eigenvalues l1 = u_n, l2 = u_n + c, l3 = u_n - c of the normal
+// velocity u_n and their positive / negative parts l+- = (l +- |l|)/2,
+//   F+- = rho/(2 gamma) [ 2(g-1) l1 + l2 + l3,
+//                         2(g-1) l1 V + l2 (V + c n) + l3 (V - c n),
+//                         (g-1) l1 |V|^2 + l2 ((u_n + c)^2 + |V_t|^2)/2 + l3 ((u_n - c)^2 + |V_t|^2)/2
+//                           + (3 - g)(l2 + l3) c^2 / (2 (g-1)) ]
+// (all l's taken +- alike), with V_t the tangential velocity.  F+ + F- is
+// the physical flux.  The reference declares this splitting
+// (field_structures.h:113-119, initialization.cpp:80-84) but implements no
+// formula, so this one has no reference output to match.
+template <int DIR, typename R>
+NS3D_HD void sw_split(const R *U, R g, R sgn, R *F) {
+    Side<DIR, R> S;
+    S.load(U, g);
+    const R c2 = g * S.p * S.ir, c = sqrt(c2);
+    auto part = [&](R l) { return R(0.5) * (l + sgn * fabs(l)); };
+    const R l1 = part(S.un), l2 = part(S.un + c), l3 = part(S.un - c);
+    const R k = S.r / (R(2) * g);
+    const R gm1 = g - R(1);
+    const R vt2 = S.u * S.u + S.v * S.v + S.w * S.w - S.un * S.un;
+    const R up = S.un + c, um = S.un - c;
+    const R m = R(2) * gm1 * l1 + l2 + l3;
+    F[0] = k * m;
+    F[1] = k * (m * S.u + (DIR == 0 ? c * (l2 - l3) : R(0)));
+    F[2] = k * (m * S.v + (DIR == 1 ? c * (l2 - l3) : R(0)));
+    F[3] = k * (m * S.w + (DIR == 2 ? c * (l2 - l3) : R(0)));
+    F[4] = k * (gm1 * l1 * (S.un * S.un + vt2) + R(0.5) * l2 * (up * up + vt2) + R(0.5) * l3 * (um * um + vt2) +
+                (R(3) - g) * (l2 + l3) * c2 / (R(2) * gm1));
+}
+
+template <int DIR, typename R>
+NS3D_HD void steger_warming_flux(const R *UL, const R *UR, R g, R *F) {
+    R Fp[5], Fm[5];
+    sw_split<DIR, R>(UL, g, R(1), Fp);
+    sw_split<DIR, R>(UR, g, R(-1), Fm);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) F[n] = Fp[n] + Fm[n];
+}
+
 template <int DIR, typename R, int RS>
 NS3D_HD void riemann(const SchemeParams<R> &sp, const R *UL, const R *UR, R *F) {
     const int rs = RS == RUNTIME ? sp.riemann : RS;
@@ -411,6 +452,8 @@ NS3D_HD void riemann(const SchemeParams<R> &sp, const R *UL, const R *UR, R *F) 
     else if (RS == R_HLL || (RS == RUNTIME && rs == R_HLL)) hll_flux<DIR, R>(UL, UR, g, F);
     else if (RS == R_HLLC_P || (RS == RUNTIME && rs == R_HLLC_P)) hllc_p_flux<DIR, R>(UL, UR, g, F);
     else if (RS == R_RUSANOV || (RS == RUNTIME && rs == R_RUSANOV)) rusanov_flux<DIR, R>(UL, UR, g, F);
+    else if (RS == R_STEGER_WARMING || (RS == RUNTIME && rs == R_STEGER_WARMING))
+        steger_warming_flux<DIR, R>(UL, UR, g, F);
     else ausm_flux<DIR, R>(UL, UR, g, F);
 }
 
