@@ -75,6 +75,15 @@ __global__ void __launch_bounds__(RED_THREADS) dt_kernel_mixed(const double *con
     block_min(m, partials + blockIdx.x);
 }
 
+// Minimum of n partials: each block of 256 threads reduces a strided share
+// into out[blockIdx.x] (a second launch with one block finishes).
+__global__ void __launch_bounds__(256) min_combine_kernel(const double *part, long n, double *out) {
+    double m = 1e9;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
+        m = fmin(m, part[t]);
+    block_min_n<256>(m, out + blockIdx.x);
+}
+
 // Non-finite / non-positive state detector: counts interior cells with a
 // non-finite value or rho <= 0 or p <= 0.
 template <typename R>
@@ -210,6 +219,9 @@ struct ns3d_handle {
     double *scratch[5] = {};   // download staging (points into a state buffer)
     double **dptr = nullptr;   // device array of pointer tables
     double *partials = nullptr;
+    double *cfl_part = nullptr;   // per-block CFL minima written by the last RK stage
+    long cfl_nblocks = 0;
+    bool cfl_valid = false;       // cfl_part describes the current state
     double *scalars = nullptr;
     int red_blocks = 0;
     bool has_state = false;
@@ -366,7 +378,8 @@ int compute_rhs_async(ns3d_handle *h) {
 // stage: 1..3 RK stages, 0 = ghost fill of the current state.
 int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double dt) {
     cudaStream_t st = h->stream;
-    dim3 g = cell_grid(h->L64, true, 128);
+    dim3 g = cell_grid(h->L64, true, STAGE_THREADS);
+    double *cfl = stage == 3 ? h->cfl_part : nullptr;  // the next step's CFL bound
     if (!h->mixed) {
         StageArgs64 a;
         for (int q = 0; q < 5; ++q) {
@@ -374,8 +387,9 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
         }
         a.L = h->L64; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
         a.Tout = h->T64; a.Rgas = h->ph.Rgas;
+        a.cfl_part = cfl; a.dx = h->ph.dx;
         prof_begin(h, "stage");
-        stage_kernel64<<<g, 128, 0, st>>>(a);
+        stage_kernel64<<<g, STAGE_THREADS, 0, st>>>(a);
         prof_end(h);
     } else {
         StageArgsMixed a;
@@ -385,12 +399,15 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
         }
         a.L = h->L64; a.L32 = h->L32; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
         a.Tout = h->T32; a.Rgas = h->ph.Rgas;
+        a.cfl_part = cfl; a.dx = h->ph.dx;
         prof_begin(h, "stage");
-        stage_kernel_mixed<<<g, 128, 0, st>>>(a);
+        stage_kernel_mixed<<<g, STAGE_THREADS, 0, st>>>(a);
         prof_end(h);
     }
     h->launches += 1;
+    h->cfl_valid = false;
     CK(h, cudaGetLastError(), "stage kernel");
+    h->cfl_valid = stage == 3;
     return NS3D_OK;
 }
 
@@ -726,6 +743,11 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     bytes += 256 * 32;                                         // pointer tables
     bytes += ((size_t)h->red_blocks * 8 * 8 + 255) / 256 * 256;  // partials
     bytes += 256;                                              // scalars
+    {
+        const dim3 sg = cell_grid(h->L64, true, STAGE_THREADS);
+        h->cfl_nblocks = (long)sg.x * sg.y * sg.z;
+    }
+    bytes += ((size_t)h->cfl_nblocks * 8 + 255) / 256 * 256;   // stage CFL minima
     cudaError_t e = cudaMalloc(&h->pool, bytes);
     if (e != cudaSuccess) { delete h; cudaGetLastError(); return NS3D_ERR_OOM; }
     h->pool_bytes = bytes;
@@ -743,7 +765,8 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     for (int q = 0; q < 9; ++q) { h->visc[q] = p; p += vis_elems * (h->mixed ? 4 : 8); }
     h->dptr = (double **)p; p += 256 * 32;
     h->partials = (double *)p; p += ((size_t)h->red_blocks * 8 * 8 + 255) / 256 * 256;
-    h->scalars = (double *)p;
+    h->scalars = (double *)p; p += 256;
+    h->cfl_part = (double *)p;
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { cudaFree(h->pool); delete h; return NS3D_ERR_CUDA; }
     h->own_stream = true;
@@ -902,6 +925,7 @@ int ns3d_upload_primitives(ns3d_handle *h, const double *const fields[5]) {
     if ((r = finish_upload(h, b, false))) return r;
     CK(h, cudaStreamSynchronize(h->stream), "synchronize");
     h->has_state = true;
+    h->cfl_valid = false;
     return NS3D_OK;
 }
 
@@ -936,6 +960,7 @@ int ns3d_set_interior_primitives(ns3d_handle *h, const double *const fields[5]) 
     if ((r = finish_upload(h, b, true))) return r;
     CK(h, cudaStreamSynchronize(h->stream), "synchronize");
     h->has_state = true;
+    h->cfl_valid = false;
     return NS3D_OK;
 }
 
@@ -1035,6 +1060,21 @@ int ns3d_compute_timestep(ns3d_handle *h, double *dt_out) {
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
     int r = set_device(h); if (r) return r;
     h->launches = 0;
+    if (h->cfl_valid) {
+        // the last RK stage left the per-block minima of this state
+        prof_begin(h, "cfl_combine");
+        const int nb = h->red_blocks;  // partials holds at least red_blocks values
+        min_combine_kernel<<<nb, 256, 0, h->stream>>>(h->cfl_part, h->cfl_nblocks, h->partials);
+        min_combine_kernel<<<1, 256, 0, h->stream>>>(h->partials, nb, h->scalars);
+        prof_end(h);
+        h->launches += 2;
+        CK(h, cudaGetLastError(), "cfl combine");
+        double m = 0;
+        CK(h, cudaMemcpyAsync(&m, h->scalars, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy dt");
+        CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+        *dt_out = h->P.cfl * m;
+        return NS3D_OK;
+    }
     prof_begin(h, "cfl_dt");
     if (!h->mixed)
         dt_kernel64<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
@@ -1179,6 +1219,7 @@ int ns3d_vjp_rk3_step(ns3d_handle *h, double dt, const double *const ubar_next[5
         for (int q = 0; q < 5; ++q)
             cudaMemcpyAsync(h->S[s_keep][q], st[0][q], bytes, cudaMemcpyDeviceToDevice, h->stream);
         h->s0 = s_keep;
+        h->cfl_valid = false;
         r = refresh_T(h);
         if (!r) r = upload_interior_slot(h, ubar_next, 0);
     }
@@ -1273,6 +1314,7 @@ int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int check
         for (int q = 0; q < 5; ++q)
             cudaMemcpyAsync(h->S[s_init][q], ck(0, q), bytes, cudaMemcpyDeviceToDevice, h->stream);
         h->s0 = s_init;
+        h->cfl_valid = false;
         AdjArgs a = adj_args(h, h->S[h->s0], h->ab[3], h->ab[0]);
         cudaError_t e = adj_velocity_grad(a, h->adj_tab, h->adj_tab + 20, h->stream);
         if (e != cudaSuccess) r = cuda_fail(h, e, "velocity gradient");

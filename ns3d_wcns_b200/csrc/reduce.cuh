@@ -47,6 +47,25 @@ __device__ __forceinline__ double block_min(double x, double *partial_out) {
     return x;
 }
 
+// Minimum over a block of NT threads (NT a multiple of 32, every thread
+// calling); thread 0 writes it.
+template <int NT>
+__device__ __forceinline__ void block_min_n(double x, double *out) {
+    __shared__ double sh[NT / 32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_down_sync(0xffffffffu, x, o));
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    if (tid == 0) {
+        double m = sh[0];
+#pragma unroll
+        for (int w = 1; w < NT / 32; ++w) m = fmin(m, sh[w]);
+        *out = m;
+    }
+}
+
 // Per-cell CFL bound of compute_timestep (timestep.cpp:12-20) from the FP64
 // conserved state: u = rhou/rho, p = (gamma-1)(E - 0.5 rho u^2) (v, w are not
 // used), a = sqrt(gamma p / rho), bound = dx / (|u| + a).

@@ -33,13 +33,26 @@ struct StageArgs64 {
     BcInfo b;
     double dt, gamma, Rgas;
     int stage;              // 1, 2, 3; 0 = ghost fill only (copy of Wc)
+    double *cfl_part;       // non-null: per-block minimum CFL bound of the new state
+    double dx;
 };
 
-__global__ void __launch_bounds__(256) stage_kernel64(StageArgs64 a) {
+constexpr int STAGE_THREADS = 128;
+
+// The CFL bound of the next step rides on the last stage: each block writes
+// the minimum of dx/(|u| + a) (timestep.cpp:12-20, from the conserved state
+// as compute_timestep sees it) over its interior cells.  The minimum of the
+// same per-cell values is the same number whatever the partition.
+__device__ __forceinline__ void stage_cfl_partial(double *cfl_part, double m) {
+    block_min_n<STAGE_THREADS>(m, cfl_part + ((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
+}
+
+__global__ void __launch_bounds__(STAGE_THREADS) stage_kernel64(StageArgs64 a) {
     const Layout &L = a.L;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
-    if (i >= L.sx) return;
+    double cfl = 1e9;  // the initial minimum of the CFL reduction kernels
+    if (i < L.sx) {
     int c[3] = {i, j, k};
     int flip;
     const int kind = resolve_source(L, a.b, c, flip);
@@ -76,6 +89,16 @@ __global__ void __launch_bounds__(256) stage_kernel64(StageArgs64 a) {
 #pragma unroll
     for (int q = 0; q < 5; ++q) a.Wout[q][o] = W[q];
     a.Tout[o] = W[4] / __dmul_rn(W[0], a.Rgas);
+    if (a.cfl_part) {
+        const int co[3] = {i, j, k};
+        if (is_interior(L, co)) {
+            double Un[5];
+            p2c_exact(W[0], W[1], W[2], W[3], W[4], a.gamma, Un);
+            cfl = cfl_bound(Un, a.gamma, a.dx);
+        }
+    }
+    }
+    if (a.cfl_part) stage_cfl_partial(a.cfl_part, cfl);
 }
 
 // --------------------------------------------------------------- mixed path
@@ -92,13 +115,16 @@ struct StageArgsMixed {
     BcInfo b;
     double dt, gamma, Rgas;
     int stage;              // 1, 2, 3; 0 = ghost fill only
+    double *cfl_part;       // non-null: per-block minimum CFL bound of the new state
+    double dx;
 };
 
-__global__ void __launch_bounds__(256) stage_kernel_mixed(StageArgsMixed a) {
+__global__ void __launch_bounds__(STAGE_THREADS) stage_kernel_mixed(StageArgsMixed a) {
     const Layout &L = a.L;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
-    if (i >= L.sx) return;
+    double cfl = 1e9;  // the initial minimum of the CFL reduction kernels
+    if (i < L.sx) {
     int c[3] = {i, j, k};
     int flip;
     const int kind = resolve_source(L, a.b, c, flip);
@@ -138,6 +164,12 @@ __global__ void __launch_bounds__(256) stage_kernel_mixed(StageArgsMixed a) {
 #pragma unroll
     for (int q = 0; q < 5; ++q) a.Wout[q][o32] = (float)W[q];
     a.Tout[o32] = (float)(W[4] / (W[0] * a.Rgas));
+    if (a.cfl_part) {
+        const int co[3] = {i, j, k};
+        if (is_interior(L, co)) cfl = cfl_bound(U, a.gamma, a.dx);
+    }
+    }
+    if (a.cfl_part) stage_cfl_partial(a.cfl_part, cfl);
 }
 
 }  // namespace ns3d

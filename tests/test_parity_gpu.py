@@ -142,3 +142,22 @@ def test_time_advance_adaptive_matches_reference_schedule(gpu_lib):
         tg, ng = s.time_advance(t_end, 100)
         assert ng == steps and tg == t
         assert per_var(s.conserved(), o.conserved()) <= STEP_TOL
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("bcs", [(0,) * 6, (3, 3, 1, 2, 0, 0)])
+def test_cfl_fused_into_last_stage(gpu_lib, precision, bcs):
+    """The time step right after an RK3 step comes from the per-block minima
+    written by the last stage; it equals the separate reduction's bit for bit."""
+    n = (20, 14, 12)
+    P, G = make_params(n=n, L=(1.0, 0.7, 0.6), interpolation=3, riemann=2, bcs=bcs, cfl=0.5, dt_fixed=-1.0,
+                       Re=300.0, precision=precision)
+    with solver(P, G) as s:
+        s.set_interior_primitives(*random_state(n, seed=5))
+        for _ in range(3):
+            dt = s.compute_timestep()
+            s.rk3_step(dt)
+            fused = s.compute_timestep()
+            s.apply_boundary()  # unchanged state, forces the separate reduction
+            plain = s.compute_timestep()
+            assert fused == plain, (fused, plain)
