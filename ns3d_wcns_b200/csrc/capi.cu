@@ -1,6 +1,8 @@
 // capi.cu -- the C ABI (include/ns3d_b200.h): handle, device memory, launch
 // sequencing of compute_rhs / runge_kutta_3 / compute_timestep /
 // compute_total_energy, and the reductions.
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -219,6 +221,10 @@ struct ns3d_handle {
     double *scratch[5] = {};   // download staging (points into a state buffer)
     double **dptr = nullptr;   // device array of pointer tables
     double *partials = nullptr;
+    int *dev_err = nullptr;       // device error word (a bounded device wait ran out)
+    // TMA tensor maps of (u, v, w) per state buffer and of T (FP64 path), or of
+    // the FP32 primitives and T (mixed path)
+    CUtensorMap tmW64[3][3], tmT64, tmW32[3], tmT32;
     double *cfl_part = nullptr;   // per-block CFL minima written by the last RK stage
     long cfl_nblocks = 0;
     bool cfl_valid = false;       // cfl_part describes the current state
@@ -323,6 +329,38 @@ SweepArgs<R> sweep_args(ns3d_handle *h, int dir) {
     return a;
 }
 
+// 3-D tensor map over one padded array (x = padded element index, y = row, z
+// = plane) with the viscous kernel's plane-tile box.
+bool encode_plane_map(CUtensorMap *m, const void *base, bool f64, const Layout &L) {
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    if (!enc) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            cudaGetLastError();
+            return false;
+        }
+        enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const cuuint64_t esz = f64 ? 8 : 4;
+    const cuuint64_t dims[3] = {(cuuint64_t)L.px, (cuuint64_t)L.sy, (cuuint64_t)L.sz};
+    const cuuint64_t strides[2] = {(cuuint64_t)L.px * esz, (cuuint64_t)L.px * L.sy * esz};
+    const cuuint32_t box[3] = {(cuuint32_t)VBX, (cuuint32_t)VBY, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base),
+               dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The plane-tile box starts at element x0 + off - 1 with x0 a multiple of 32:
+// its byte offset must be a multiple of 16 (a TMA rule nothing checks at run
+// time), as must the row pitch.
+bool plane_box_aligned(const Layout &L, size_t esz) {
+    return ((size_t)(L.off - 1) * esz) % 16 == 0 && ((size_t)VTX * esz) % 16 == 0 &&
+           ((size_t)L.px * esz) % 16 == 0 && L.off >= 1;
+}
+
 template <typename R>
 ViscArgs<R> visc_args(ns3d_handle *h) {
     ViscArgs<R> a;
@@ -341,6 +379,7 @@ ViscArgs<R> visc_args(ns3d_handle *h) {
         a.dinv[d][2] = (R)(1.0 / (60.0 * hh[d]));
     }
     a.mu0 = (R)h->ph.mu; a.S = (R)h->ph.S;
+    a.err = h->dev_err;
     a.cp_over_pr = (R)(h->ph.Cp / h->ph.Pr);
     return a;
 }
@@ -352,8 +391,11 @@ int rhs_impl(ns3d_handle *h) {
     if (h->ph.mu != 0.0) {  // Re = inf: the viscous terms are exactly zero
         ViscArgs<R> va = visc_args<R>(h);
         dim3 g((va.L.nx + VTX - 1) / VTX, (va.L.ny + VTY - 1) / VTY, (va.L.nz + VZC - 1) / VZC);
+        ViscMaps maps;
+        for (int q = 0; q < 3; ++q) maps.m[q] = sizeof(R) == 8 ? h->tmW64[h->s0][q] : h->tmW32[q];
+        maps.m[3] = sizeof(R) == 8 ? h->tmT64 : h->tmT32;
         prof_begin(h, "viscous_flux");
-        viscous_flux_kernel<R><<<g, dim3(VTX, VTY), 0, st>>>(va);
+        viscous_flux_kernel<R><<<g, dim3(VTX, VTY), 0, st>>>(va, maps);
         prof_end(h);
         h->launches += 1;
         CK(h, cudaGetLastError(), "viscous kernel");
@@ -765,7 +807,9 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     for (int q = 0; q < 9; ++q) { h->visc[q] = p; p += vis_elems * (h->mixed ? 4 : 8); }
     h->dptr = (double **)p; p += 256 * 32;
     h->partials = (double *)p; p += ((size_t)h->red_blocks * 8 * 8 + 255) / 256 * 256;
-    h->scalars = (double *)p; p += 256;
+    h->scalars = (double *)p;
+    h->dev_err = (int *)((char *)p + 128);
+    p += 256;
     h->cfl_part = (double *)p;
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { cudaFree(h->pool); delete h; return NS3D_ERR_CUDA; }
@@ -780,7 +824,25 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     }
     e = cudaMemcpy(h->dptr, tab, sizeof(tab), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->pool, 0, (size_t)((char *)h->dptr - (char *)h->pool));
+    if (e == cudaSuccess) e = cudaMemset(h->dev_err, 0, sizeof(int));
     if (e != cudaSuccess) { ns3d_destroy(h); return NS3D_ERR_CUDA; }
+    // TMA tensor maps of the viscous kernel's plane tiles
+    {
+        bool ok = plane_box_aligned(h->mixed ? h->L32 : h->L64, h->mixed ? 4 : 8);
+        if (!h->mixed) {
+            for (int b = 0; b < 3 && ok; ++b)
+                for (int q = 0; q < 3 && ok; ++q) ok = encode_plane_map(&h->tmW64[b][q], h->S[b][q + 1], true, h->L64);
+            if (ok) ok = encode_plane_map(&h->tmT64, h->T64, true, h->L64);
+        } else {
+            for (int q = 0; q < 3 && ok; ++q) ok = encode_plane_map(&h->tmW32[q], h->w32[q + 1], false, h->L32);
+            if (ok) ok = encode_plane_map(&h->tmT32, h->T32, false, h->L32);
+        }
+        if (!ok) {
+            ns3d_destroy(h);
+            g_create_error = "TMA tensor maps of the viscous tiles could not be encoded";
+            return NS3D_ERR_CUDA;
+        }
+    }
     // Field3D::allocate: rho = 1 everywhere (field_structures.h:257)
     for (int b = 0; b < 3; ++b) {
         fill_kernel<double><<<256, 256, 0, h->stream>>>(h->S[b][0], h->L64.plane, 1.0);
@@ -1017,13 +1079,28 @@ int ns3d_apply_boundary(ns3d_handle *h) {
     return NS3D_OK;
 }
 
+int check_device_error(ns3d_handle *h);
+
 int ns3d_compute_rhs(ns3d_handle *h) {
     if (!h) return NS3D_ERR_INVALID_ARG;
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
     int r = set_device(h); if (r) return r;
     h->launches = 0;
     if ((r = compute_rhs_async(h))) return r;
+    return check_device_error(h);
+}
+
+// The kernels' bounded waits record a non-zero error word instead of
+// spinning for ever; read it after the work of an entry point.
+int check_device_error(ns3d_handle *h) {
+    int code = 0;
+    CK(h, cudaMemcpyAsync(&code, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "error word");
     CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    if (code) {
+        cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream);
+        return fail(h, NS3D_ERR_TIMEOUT, "a device-side wait for a TMA tile ran out (error word " +
+                                             std::to_string(code) + ")");
+    }
     return NS3D_OK;
 }
 
@@ -1034,8 +1111,8 @@ int ns3d_rk3_step(ns3d_handle *h, double dt) {
     int r = set_device(h); if (r) return r;
     h->launches = 0;
     if ((r = rk3_async(h, dt))) return r;
+    if ((r = check_device_error(h))) return r;
     if (h->P.check_state) return check_state(h);
-    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
     return NS3D_OK;
 }
 
@@ -1050,8 +1127,8 @@ int ns3d_rk3_steps(ns3d_handle *h, int nsteps, double dt) {
     for (int s = 0; s < nsteps; ++s) {
         if ((r = rk3_async(h, dt))) return r;
     }
+    if ((r = check_device_error(h))) return r;
     if (h->P.check_state) return check_state(h);
-    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
     return NS3D_OK;
 }
 

@@ -8,7 +8,8 @@
 // (compute_viscous_flux, ViscousFlux.cpp:151-208; F_v = (txx,txy,txz,ex),
 // H_v = (txy,tyy,tyz,ey), G_v = (txz,tyz,tzz,ez)).
 //
-// A block owns a 32 x 8 column of nodes and marches along z (see the kernel).
+// A block owns a 32 x 8 column of nodes and marches along z; the plane tiles
+// with their halo arrive by TMA (see the kernel).
 // T is the array the stage kernel stores (p/(rho Rgas)).
 //
 // The divergence of these fluxes (compute_vis_flux, ViscousFlux.cpp:210-255)
@@ -20,6 +21,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace ns3d {
 
@@ -33,6 +35,7 @@ struct ViscArgs {
     R h[3];
     R dinv[3][3];           // per direction: 1/(2h), 1/(12h), 1/(60h)
     R mu0, S, cp_over_pr;
+    int *err;               // device error word (a bounded wait that ran out)
 };
 
 // choose_scheme, ViscousFlux.cpp:33-50 (idx relative to the first interior node)
@@ -90,40 +93,60 @@ __device__ __forceinline__ R dtile(F f, int order, const R *dinv) {
 
 // A block owns a 32 x 8 column of nodes and marches up VZC planes: each
 // thread keeps its node's (u, v, w, T) of planes k-3 .. k+3 in registers and
-// loads one new plane per step; the x/y derivatives read the plane's tile
-// (with its 3-cell halo) from shared memory.  Every input value is read from
-// memory about once per use plane instead of once per neighbour.
+// loads one new plane per step (prefetched a step ahead); the x/y derivatives
+// read the plane's tile with its 3-cell halo, which one thread requests as
+// four TMA boxes a plane ahead (double buffer, mbarrier completion, bounded
+// waits).
+// Tensor maps of u, v, w, T of the state being differenced (3-D: x = padded
+// element index, y = ghost-inclusive row, z = ghost-inclusive plane).
+struct ViscMaps {
+    CUtensorMap m[4];
+};
+
+// Plane tile as loaded by TMA: rows y0 .. y0+13 (ghost-inclusive), elements
+// x0 + off - 1 .. x0 + off + 38 of each row, so a node's ghost-inclusive x0 + t
+// sits in column t + 1.  Starting one element early puts the box's x
+// coordinate on a 16-byte boundary for both element sizes (FP64: off = 1,
+// FP32: off = 5).
+constexpr int VBX = 40, VBY = VTY + 2 * VH;
 template <typename R>
-__global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a) {
-    // two plane tiles: the next plane's tile is copied (cp.async) while the
-    // current one is differenced
-    __shared__ __align__(16) R sm[2][4][VTY + 2 * VH][VTX + 2 * VH];
+constexpr int vtile_stride() {  // elements per tile, 128-byte aligned tiles
+    return (int)(((VBX * VBY * sizeof(R) + 127) / 128) * 128 / sizeof(R));
+}
+
+template <typename R>
+__global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, const __grid_constant__ ViscMaps tm) {
+    constexpr int TS = vtile_stride<R>();
+    __shared__ __align__(128) R sm[2 * 4 * TS];  // two plane tiles of u, v, w, T
+    __shared__ __align__(8) uint64_t bar[2];
     const Layout &L = a.L;
     const int x0 = blockIdx.x * VTX, y0 = blockIdx.y * VTY;
     const int kb = blockIdx.z * VZC, ke = min(kb + VZC, L.nz);
     const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
+    const int tid = threadIdx.y * VTX + threadIdx.x;
     const bool in = i < L.nx && j < L.ny;
     const R *src[4] = {a.W[1], a.W[2], a.W[3], a.T};
     const long zs = (long)L.px * L.sy;
     const long col = L.at(min(i, L.nx - 1) + NG, min(j, L.ny - 1) + NG, 0);  // ghost-inclusive plane 0
     const int ox = visc_order(i, L.nx, a.periodic[0]);
     const int oy = visc_order(j, L.ny, a.periodic[1]);
-    const int cx = threadIdx.x + VH, cy = threadIdx.y + VH;
-    auto fetch_tile = [&](int buf, int k) {  // plane k (interior index), ghost-inclusive x/y
-        for (int t = threadIdx.y * VTX + threadIdx.x; t < (VTX + 2 * VH) * (VTY + 2 * VH); t += VTX * VTY) {
-            const int tx = t % (VTX + 2 * VH), ty = t / (VTX + 2 * VH);
-            const int gx = x0 + tx, gy = y0 + ty;
-            if (gx < L.sx && gy < L.sy) {
-                const long id = L.at(gx, gy, k + NG);
+    const int cx = threadIdx.x + VH + 1, cy = threadIdx.y + VH;
+    auto tile = [&](int buf, int q) { return sm + (buf * 4 + q) * TS; };
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto issue = [&](int buf, int k) {  // one thread: four boxes of plane k
+        mbar_arrive_expect_tx(&bar[buf], 4u * VBX * VBY * (unsigned)sizeof(R));
 #pragma unroll
-                for (int q = 0; q < 4; ++q) cp_async(&sm[buf][q][ty][tx], src[q] + id);
-            }
-        }
-        cp_async_commit();
+        for (int q = 0; q < 4; ++q) tma_load_3d(tile(buf, q), &tm.m[q], x0 + L.off - 1, y0, k + NG, &bar[buf]);
     };
+    unsigned phase = 0u;  // bit b: parity of buffer b's next completion
+    if (tid == 0) issue(0, kb);
     // window: win[q][m] = value at interior plane k - 3 + m (ghost-inclusive k + m)
     R win[4][7], nxt[4];
-    fetch_tile(0, kb);
 #pragma unroll
     for (int m = 0; m < 6; ++m)
 #pragma unroll
@@ -133,22 +156,33 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a) 
     for (int k = kb; k < ke; ++k) {
         const int buf = (k - kb) & 1;
         const bool more = k + 1 < ke;
-        if (more) fetch_tile(buf ^ 1, k + 1);
+        if (more && tid == 0) {
+            fence_proxy_async_smem();  // the tile's last readers finished at the previous barrier
+            issue(buf ^ 1, k + 1);
+        }
 #pragma unroll
         for (int q = 0; q < 4; ++q) win[q][6] = nxt[q];
         if (more) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) nxt[q] = src[q][col + (long)(k + 7) * zs];
         }
-        if (more) cp_async_wait<1>(); else cp_async_wait<0>();  // this plane's tile landed
-        __syncthreads();
+        const bool ok = mbar_wait_bounded(&bar[buf], (phase >> buf) & 1u, a.err);
+        phase ^= 1u << buf;
+        if (__syncthreads_or(!ok)) {
+            // a tile never arrived: let the other copy (if any) land, bounded, and stop
+            if (more && tid == 0) mbar_wait_bounded(&bar[buf ^ 1], (phase >> (buf ^ 1)) & 1u, a.err);
+            return;
+        }
         if (in) {
+            const R *tu = tile(buf, 0), *tv = tile(buf, 1), *tw = tile(buf, 2), *tT = tile(buf, 3);
+            const R *tq[4] = {tu, tv, tw, tT};
             const int oz = visc_order(k, L.nz, a.periodic[2]);
             R g[4][3];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                g[q][0] = dtile<R>([&](int o) { return sm[buf][q][cy][cx + o]; }, ox, a.dinv[0]);
-                g[q][1] = dtile<R>([&](int o) { return sm[buf][q][cy + o][cx]; }, oy, a.dinv[1]);
+                const R *t = tq[q];
+                g[q][0] = dtile<R>([&](int o) { return t[cy * VBX + cx + o]; }, ox, a.dinv[0]);
+                g[q][1] = dtile<R>([&](int o) { return t[(cy + o) * VBX + cx]; }, oy, a.dinv[1]);
                 g[q][2] = dwindow<R>([&](int o) { return win[q][3 + o]; }, oz, a.dinv[2]);
             }
             const R T = win[3][3];
