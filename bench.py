@@ -188,7 +188,8 @@ def adjoint_report(device: int, n: int = 64, nsteps: int = 200, dt: float = 2e-3
         J, grad, stats = s.adjoint_kinetic_energy(nsteps, dt, ce)
         s.set_interior_primitives(*st)
         J2, grad2, stats2 = s.adjoint_kinetic_energy(nsteps, dt, ce)  # warm timing
-        errs, errs4, noise = [], [], []
+        errs, errs4, noise, errsn = [], [], [], []
+        gnorm = float(np.sqrt(np.sum(grad2 * grad2)))
         h = 1e-6
 
         def J_at(eps, d):
@@ -207,6 +208,7 @@ def adjoint_report(device: int, n: int = 64, nsteps: int = 200, dt: float = 2e-3
             ad = float(np.sum(grad2 * d))
             errs.append(abs(fd - ad) / abs(fd))
             errs4.append(abs(fd4 - ad) / abs(fd4))
+            errsn.append(abs(fd - ad) / (gnorm * float(np.sqrt(np.sum(d * d)))))
             noise.append(abs(fd - fd2) / abs(fd))   # size of the FD's own error
     return {"config": f"{n}^3 isotropic WENO5+Roe, Re 200, dt {dt}, {nsteps} steps, checkpoint every {ce}",
             "J": J2, "forward_ms": stats2["forward_ms"], "adjoint_ms": stats2["adjoint_ms"],
@@ -214,7 +216,9 @@ def adjoint_report(device: int, n: int = 64, nsteps: int = 200, dt: float = 2e-3
             "peak_adjoint_bytes": stats2["adjoint_bytes"], "fd_directions": ndir, "fd_h": 1e-6,
             "fd_max_rel_err": max(errs), "fd_median_rel_err": float(np.median(errs)),
             "fd4_max_rel_err": max(errs4), "fd4_median_rel_err": float(np.median(errs4)),
-            "fd_h_vs_2h_max_rel": max(noise), "recomputed_steps": stats2["recomputed_steps"],
+            "fd_h_vs_2h_max_rel": max(noise),
+            "fd_max_err_over_grad_norm": max(errsn),  # |fd - ad| / (|grad| |d|)
+            "recomputed_steps": stats2["recomputed_steps"],
             "forward_pass_includes": "checkpoint copies and the last segment's stage-state copies"}
 
 

@@ -252,6 +252,13 @@ int ns3d_debug_visc_vjp(double mu0, double S, double cp_over_pr, const double *x
  * InviscousFlux.cpp:270-846); for unit tests of the flux functions. */
 int ns3d_debug_riemann(int direction, int riemann, double gamma, const double UL[5], const double UR[5],
                        double F[5]);
+/* Runs the bounded mbarrier wait of the TMA kernels against a barrier that
+ * never completes (armed for bytes no copy delivers): each block gives up
+ * after `polls` polls, writes the device error word (returned in *code_out)
+ * and exits.  Returns NS3D_ERR_TIMEOUT when that happened, as the solver
+ * entry points do when one of their TMA waits runs out.  No counterpart in
+ * the reference; for tests of the failure path. */
+int ns3d_debug_wait_timeout(int device, unsigned polls, int *code_out);
 
 /* ---------------------------------------- scratch-free CFL time step
  * No counterpart in the reference.  For host codes that cannot let a library

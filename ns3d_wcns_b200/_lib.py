@@ -27,7 +27,7 @@ EXPORTS = [
     "ns3d_compute_timestep", "ns3d_total_energy", "ns3d_diagnostics", "ns3d_time_advance",
     "ns3d_device_fields", "ns3d_set_stream", "ns3d_synchronize", "ns3d_last_launch_count",
     "ns3d_profile", "ns3d_profile_report", "ns3d_compute_timestep_noalloc",
-    "ns3d_debug_face_vjp", "ns3d_debug_visc_vjp", "ns3d_debug_riemann", "ns3d_vjp_rhs", "ns3d_vjp_rk3_step",
+    "ns3d_debug_face_vjp", "ns3d_debug_visc_vjp", "ns3d_debug_riemann", "ns3d_debug_wait_timeout", "ns3d_vjp_rhs", "ns3d_vjp_rk3_step",
     "ns3d_adjoint_kinetic_energy", "ns3d_batch_create", "ns3d_batch_destroy", "ns3d_batch_last_error",
     "ns3d_batch_set_interior_primitives", "ns3d_batch_run", "ns3d_batch_autotune", "ns3d_batch_set_config",
     "ns3d_batch_query", "ns3d_batch_download",
@@ -107,6 +107,7 @@ def load() -> C.CDLL:
     lib.ns3d_debug_face_vjp.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, dp]
     lib.ns3d_debug_visc_vjp.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp]
     lib.ns3d_debug_riemann.argtypes = [C.c_int, C.c_int, C.c_double, dp, dp, dp]
+    lib.ns3d_debug_wait_timeout.argtypes = [C.c_int, C.c_uint, C.POINTER(C.c_int)]
     lib.ns3d_compute_timestep_noalloc.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_double,
                                                   C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     _lib = lib

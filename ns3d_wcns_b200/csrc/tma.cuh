@@ -52,8 +52,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
 }
 
 // bounded wait; false (and the error word set) when the limit ran out
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, int *err) {
-    for (unsigned it = 0; it < TMA_SPIN_LIMIT; ++it)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, int *err,
+                                                  unsigned limit = TMA_SPIN_LIMIT) {
+    for (unsigned it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     if (err) atomicExch(err, NS3D_DEVERR_TMA_TIMEOUT);
     return false;
