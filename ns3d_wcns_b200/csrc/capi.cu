@@ -77,6 +77,16 @@ __global__ void __launch_bounds__(RED_THREADS) dt_kernel_mixed(const double *con
     block_min(m, partials + blockIdx.x);
 }
 
+// Sum of n partials, deterministic: each block of 256 threads sums a strided
+// share into out[blockIdx.x] in a fixed order (a second launch with one block
+// finishes).
+__global__ void __launch_bounds__(256) sum_combine_kernel(const double *part, long n, double *out) {
+    double s = 0.0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) s += part[t];
+    double v[1] = {s};
+    block_sum<1>(v, out + blockIdx.x);
+}
+
 // Minimum of n partials: each block of 256 threads reduces a strided share
 // into out[blockIdx.x] (a second launch with one block finishes).
 __global__ void __launch_bounds__(256) min_combine_kernel(const double *part, long n, double *out) {
@@ -226,6 +236,7 @@ struct ns3d_handle {
     // the FP32 primitives and T (mixed path)
     CUtensorMap tmW64[3][3], tmT64, tmW32[3], tmT32;
     double *cfl_part = nullptr;   // per-block CFL minima written by the last RK stage
+    double *ke_part = nullptr;    // per-block kinetic energy written by the last RK stage
     long cfl_nblocks = 0;
     bool cfl_valid = false;       // cfl_part describes the current state
     double *scalars = nullptr;
@@ -429,7 +440,8 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
         }
         a.L = h->L64; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
         a.Tout = h->T64; a.Rgas = h->ph.Rgas;
-        a.cfl_part = cfl; a.dx = h->ph.dx;
+        a.cfl_part = cfl; a.ke_part = h->ke_part; a.dx = h->ph.dx;
+        a.vol = h->ph.dx * h->ph.dy * h->ph.dz;
         prof_begin(h, "stage");
         stage_kernel64<<<g, STAGE_THREADS, 0, st>>>(a);
         prof_end(h);
@@ -441,7 +453,8 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
         }
         a.L = h->L64; a.L32 = h->L32; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
         a.Tout = h->T32; a.Rgas = h->ph.Rgas;
-        a.cfl_part = cfl; a.dx = h->ph.dx;
+        a.cfl_part = cfl; a.ke_part = h->ke_part; a.dx = h->ph.dx;
+        a.vol = h->ph.dx * h->ph.dy * h->ph.dz;
         prof_begin(h, "stage");
         stage_kernel_mixed<<<g, STAGE_THREADS, 0, st>>>(a);
         prof_end(h);
@@ -789,7 +802,7 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
         const dim3 sg = cell_grid(h->L64, true, STAGE_THREADS);
         h->cfl_nblocks = (long)sg.x * sg.y * sg.z;
     }
-    bytes += ((size_t)h->cfl_nblocks * 8 + 255) / 256 * 256;   // stage CFL minima
+    bytes += 2 * (((size_t)h->cfl_nblocks * 8 + 255) / 256 * 256);  // stage CFL minima, kinetic energy
     cudaError_t e = cudaMalloc(&h->pool, bytes);
     if (e != cudaSuccess) { delete h; cudaGetLastError(); return NS3D_ERR_OOM; }
     h->pool_bytes = bytes;
@@ -811,6 +824,8 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     h->dev_err = (int *)((char *)p + 128);
     p += 256;
     h->cfl_part = (double *)p;
+    p += ((size_t)h->cfl_nblocks * 8 + 255) / 256 * 256;
+    h->ke_part = (double *)p;
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { cudaFree(h->pool); delete h; return NS3D_ERR_CUDA; }
     h->own_stream = true;
@@ -1209,7 +1224,20 @@ int ns3d_diagnostics(ns3d_handle *h, double out[6]) {
 }
 
 int ns3d_total_energy(ns3d_handle *h, double *ke_out) {
-    if (!ke_out) return NS3D_ERR_INVALID_ARG;
+    if (!h || !ke_out) return NS3D_ERR_INVALID_ARG;
+    if (h->cfl_valid) {
+        // the last RK stage left the per-block kinetic energies of this state
+        int r = set_device(h); if (r) return r;
+        h->launches = 0;
+        const int nb = h->red_blocks;
+        sum_combine_kernel<<<nb, 256, 0, h->stream>>>(h->ke_part, h->cfl_nblocks, h->partials);
+        sum_combine_kernel<<<1, 256, 0, h->stream>>>(h->partials, nb, h->scalars);
+        h->launches += 2;
+        CK(h, cudaGetLastError(), "kinetic energy combine");
+        CK(h, cudaMemcpyAsync(ke_out, h->scalars, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy energy");
+        CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+        return NS3D_OK;
+    }
     double d[6];
     int r = ns3d_diagnostics(h, d);
     if (r) return r;

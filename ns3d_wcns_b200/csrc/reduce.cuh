@@ -66,6 +66,29 @@ __device__ __forceinline__ void block_min_n(double x, double *out) {
     }
 }
 
+// Minimum of m and sum of v over a block of NT threads (NT a multiple of 32,
+// every thread calling), in a fixed order; thread 0 writes both.
+template <int NT>
+__device__ __forceinline__ void block_min_sum_n(double m, double v, double *out_min, double *out_sum) {
+    __shared__ double shm[NT / 32], shs[NT / 32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    if (lane == 0) { shm[wid] = m; shs[wid] = v; }
+    __syncthreads();
+    if (tid == 0) {
+        double a = shm[0], b = shs[0];
+#pragma unroll
+        for (int w = 1; w < NT / 32; ++w) { a = fmin(a, shm[w]); b += shs[w]; }
+        *out_min = a;
+        *out_sum = b;
+    }
+}
+
 // Per-cell CFL bound of compute_timestep (timestep.cpp:12-20) from the FP64
 // conserved state: u = rhou/rho, p = (gamma-1)(E - 0.5 rho u^2) (v, w are not
 // used), a = sqrt(gamma p / rho), bound = dx / (|u| + a).

@@ -34,17 +34,21 @@ struct StageArgs64 {
     double dt, gamma, Rgas;
     int stage;              // 1, 2, 3; 0 = ghost fill only (copy of Wc)
     double *cfl_part;       // non-null: per-block minimum CFL bound of the new state
-    double dx;
+    double *ke_part;        // with cfl_part: per-block kinetic energy of the new state
+    double dx, vol;
 };
 
 constexpr int STAGE_THREADS = 128;
 
-// The CFL bound of the next step rides on the last stage: each block writes
-// the minimum of dx/(|u| + a) (timestep.cpp:12-20, from the conserved state
-// as compute_timestep sees it) over its interior cells.  The minimum of the
-// same per-cell values is the same number whatever the partition.
-__device__ __forceinline__ void stage_cfl_partial(double *cfl_part, double m) {
-    block_min_n<STAGE_THREADS>(m, cfl_part + ((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
+// The CFL bound of the next step and the kinetic energy of the new state
+// ride on the last stage: each block writes the minimum of dx/(|u| + a)
+// (timestep.cpp:12-20, from the conserved state as compute_timestep sees it)
+// and the sum of rho |u|^2 / 2 dV (postprocess.cpp:103-128) over its interior
+// cells.  The minimum of the same per-cell values is the same number whatever
+// the partition; the sum is fixed-order (deterministic).
+__device__ __forceinline__ void stage_partials(double *cfl_part, double *ke_part, double m, double ke) {
+    const long b = ((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    block_min_sum_n<STAGE_THREADS>(m, ke, cfl_part + b, ke_part + b);
 }
 
 __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel64(StageArgs64 a) {
@@ -52,6 +56,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel64(StageArgs64 a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     double cfl = 1e9;  // the initial minimum of the CFL reduction kernels
+    double ke = 0.0;
     if (i < L.sx) {
     int c[3] = {i, j, k};
     int flip;
@@ -95,10 +100,11 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel64(StageArgs64 a) {
             double Un[5];
             p2c_exact(W[0], W[1], W[2], W[3], W[4], a.gamma, Un);
             cfl = cfl_bound(Un, a.gamma, a.dx);
+            ke = 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * a.vol;
         }
     }
     }
-    if (a.cfl_part) stage_cfl_partial(a.cfl_part, cfl);
+    if (a.cfl_part) stage_partials(a.cfl_part, a.ke_part, cfl, ke);
 }
 
 // --------------------------------------------------------------- mixed path
@@ -116,7 +122,8 @@ struct StageArgsMixed {
     double dt, gamma, Rgas;
     int stage;              // 1, 2, 3; 0 = ghost fill only
     double *cfl_part;       // non-null: per-block minimum CFL bound of the new state
-    double dx;
+    double *ke_part;        // with cfl_part: per-block kinetic energy of the new state
+    double dx, vol;
 };
 
 __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel_mixed(StageArgsMixed a) {
@@ -124,6 +131,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel_mixed(StageArgsMix
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     double cfl = 1e9;  // the initial minimum of the CFL reduction kernels
+    double ke = 0.0;
     if (i < L.sx) {
     int c[3] = {i, j, k};
     int flip;
@@ -166,10 +174,13 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel_mixed(StageArgsMix
     a.Tout[o32] = (float)(W[4] / (W[0] * a.Rgas));
     if (a.cfl_part) {
         const int co[3] = {i, j, k};
-        if (is_interior(L, co)) cfl = cfl_bound(U, a.gamma, a.dx);
+        if (is_interior(L, co)) {
+            cfl = cfl_bound(U, a.gamma, a.dx);
+            ke = 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * a.vol;
+        }
     }
     }
-    if (a.cfl_part) stage_cfl_partial(a.cfl_part, cfl);
+    if (a.cfl_part) stage_partials(a.cfl_part, a.ke_part, cfl, ke);
 }
 
 }  // namespace ns3d

@@ -148,7 +148,8 @@ def test_time_advance_adaptive_matches_reference_schedule(gpu_lib):
 @pytest.mark.parametrize("bcs", [(0,) * 6, (3, 3, 1, 2, 0, 0)])
 def test_cfl_fused_into_last_stage(gpu_lib, precision, bcs):
     """The time step right after an RK3 step comes from the per-block minima
-    written by the last stage; it equals the separate reduction's bit for bit."""
+    written by the last stage; it equals the separate reduction's bit for bit.
+    The kinetic energy of the new state comes from the same stage's block sums."""
     n = (20, 14, 12)
     P, G = make_params(n=n, L=(1.0, 0.7, 0.6), interpolation=3, riemann=2, bcs=bcs, cfl=0.5, dt_fixed=-1.0,
                        Re=300.0, precision=precision)
@@ -158,6 +159,10 @@ def test_cfl_fused_into_last_stage(gpu_lib, precision, bcs):
             dt = s.compute_timestep()
             s.rk3_step(dt)
             fused = s.compute_timestep()
-            s.apply_boundary()  # unchanged state, forces the separate reduction
+            ke_fused = s.total_energy()
+            s.apply_boundary()  # unchanged state, forces the separate reductions
             plain = s.compute_timestep()
             assert fused == plain, (fused, plain)
+            # kinetic energy: the same sum in another (fixed) order
+            ke_plain = s.total_energy()
+            assert abs(ke_fused - ke_plain) <= 1e-13 * abs(ke_plain), (ke_fused, ke_plain)
