@@ -28,6 +28,14 @@ def _torch():
     return torch
 
 
+def _t(x, device):
+    """float64 torch tensor on `device` (zero-copy for a tensor already there)."""
+    torch = _torch()
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=torch.float64)
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=torch.float64, device=device)
+
+
 def energy_spectrum(u, v, w, device: str = "cpu") -> np.ndarray:
     """Shell spectrum E(k), k = 0..2*NX (EnergySpectrum.cpp:63-135)."""
     torch = _torch()
@@ -35,11 +43,10 @@ def energy_spectrum(u, v, w, device: str = "cpu") -> np.ndarray:
     N = nx * ny * nz
     er = None
     for f in (u, v, w):
-        t = torch.as_tensor(np.ascontiguousarray(f), dtype=torch.float64, device=device)
-        h = torch.fft.fftn(t) / N
+        h = torch.fft.fftn(_t(f, device).contiguous()) / N
         e = (h.real * h.real + h.imag * h.imag)
         er = e if er is None else er + e
-        del t, h
+        del h
     er = er * 0.5
 
     def wav(n):
@@ -58,12 +65,14 @@ def energy_spectrum(u, v, w, device: str = "cpu") -> np.ndarray:
 
 def sutherland_mu(T, mu0: float, S: float):
     """mu(T) = mu0 T^1.5 (1 + S)/(T + S) (field_structures.h:96-106)."""
-    return mu0 * np.power(T, 1.5) * (1.0 + S) / (T + S)
+    return mu0 * T ** 1.5 * (1.0 + S) / (T + S)
 
 
 def turbulence_stats(rho, u, v, w, T, mu0: float, S: float, dV: float, device: str = "cpu") -> Dict:
-    """Kinetic energy, u_rms, nu and the spectral dissipation of ana_isotropic.cpp:230-305."""
-    N = rho.size
+    """Kinetic energy, u_rms, nu and the spectral dissipation of ana_isotropic.cpp:230-305.
+    Inputs: numpy arrays or torch tensors (used in place when already on `device`)."""
+    rho, u, v, w, T = (_t(x, device) for x in (rho, u, v, w, T))
+    N = rho.numel()
     q = u * u + v * v + w * w
     mean_mu = float(sutherland_mu(T, mu0, S).sum()) / N
     mean_rho = float(rho.sum()) / N
@@ -71,10 +80,11 @@ def turbulence_stats(rho, u, v, w, T, mu0: float, S: float, dV: float, device: s
     Ek = energy_spectrum(u, v, w, device)
     k = np.arange(Ek.size, dtype=np.float64)
     eps = float(np.sum(2.0 * nu * k * k * Ek))
+    qs = float(q.sum())
     return {
-        "total_energy": float(0.5 * (rho * q).sum() * dV),   # postprocess.cpp:103-128
-        "kinetic_energy": float(0.5 * q.sum()) / N,           # ana_isotropic.cpp:280
-        "u_rms": math.sqrt(float(q.sum()) / (3.0 * N)),
+        "total_energy": float(0.5 * (rho * q).sum()) * dV,    # postprocess.cpp:103-128
+        "kinetic_energy": 0.5 * qs / N,                        # ana_isotropic.cpp:280
+        "u_rms": math.sqrt(qs / (3.0 * N)),
         "mean_mu": mean_mu, "mean_rho": mean_rho, "nu": nu,
         "dissipation": eps, "spectrum": Ek,
     }

@@ -87,6 +87,29 @@ __global__ void __launch_bounds__(256) sum_combine_kernel(const double *part, lo
     block_sum<1>(v, out + blockIdx.x);
 }
 
+// One step of time_advance's dt schedule (maincycle.cpp:18-56) on the
+// device, same operations as the host loop: stop when |t_end - t| <= eps, when
+// the previous step reached t_end or when the step budget is spent; dt from the
+// CFL minimum (adaptive) or dt_fixed, clipped to t_end; dt <= eps is the
+// reference's error.
+__global__ void schedule_kernel(DevClock *c, double cfl, double dt_fixed, double eps) {
+    if (c->done) return;
+    if (c->steps >= c->budget || fabs(c->t_end - c->t) <= eps || (c->steps > 0 && c->t >= c->t_end)) {
+        c->done = 1;
+        return;
+    }
+    double dt = dt_fixed >= 0.0 ? dt_fixed : cfl * c->cfl_min;
+    if (c->t + dt > c->t_end) dt = c->t_end - c->t;
+    if (dt <= eps) {
+        c->done = 1;
+        c->err = 1;
+        return;
+    }
+    c->t += dt;
+    c->dt = dt;
+    c->steps += 1;
+}
+
 // Minimum of n partials: each block of 256 threads reduces a strided share
 // into out[blockIdx.x] (a second launch with one block finishes).
 __global__ void __launch_bounds__(256) min_combine_kernel(const double *part, long n, double *out) {
@@ -244,7 +267,9 @@ struct ns3d_handle {
     bool has_state = false;
     long launches = 0;
     std::string err;
-    cudaGraphExec_t step_graph = nullptr;
+    DevClock *clock = nullptr;           // device time-advance state
+    bool dev_loop = false;               // kernels being captured read dt / done from clock
+    cudaGraphExec_t adv_graph[3] = {};   // ADV_STEPS steps, per starting buffer rotation
     double graph_dt = 0.0;
     int graph_s0 = -1;
     // per-kernel CUDA-event timing (ns3d_profile)
@@ -337,6 +362,7 @@ SweepArgs<R> sweep_args(ns3d_handle *h, int dir) {
     // node fluxes of this direction for rhou, rhov, rhow, E: F_v, H_v, G_v
     static const int comp[3][4] = {{0, 3, 4, 6}, {3, 1, 5, 7}, {4, 5, 2, 8}};
     for (int q = 0; q < 4; ++q) a.V[q] = (const R *)h->visc[comp[dir][q]];
+    a.done = h->dev_loop ? &h->clock->done : nullptr;
     return a;
 }
 
@@ -391,6 +417,7 @@ ViscArgs<R> visc_args(ns3d_handle *h) {
     }
     a.mu0 = (R)h->ph.mu; a.S = (R)h->ph.S;
     a.err = h->dev_err;
+    a.done = h->dev_loop ? &h->clock->done : nullptr;
     a.cp_over_pr = (R)(h->ph.Cp / h->ph.Pr);
     return a;
 }
@@ -442,6 +469,8 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
         a.Tout = h->T64; a.Rgas = h->ph.Rgas;
         a.cfl_part = cfl; a.ke_part = h->ke_part; a.dx = h->ph.dx;
         a.vol = h->ph.dx * h->ph.dy * h->ph.dz;
+        a.dt_dev = h->dev_loop ? &h->clock->dt : nullptr;
+        a.done = h->dev_loop ? &h->clock->done : nullptr;
         prof_begin(h, "stage");
         stage_kernel64<<<g, STAGE_THREADS, 0, st>>>(a);
         prof_end(h);
@@ -455,6 +484,8 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
         a.Tout = h->T32; a.Rgas = h->ph.Rgas;
         a.cfl_part = cfl; a.ke_part = h->ke_part; a.dx = h->ph.dx;
         a.vol = h->ph.dx * h->ph.dy * h->ph.dz;
+        a.dt_dev = h->dev_loop ? &h->clock->dt : nullptr;
+        a.done = h->dev_loop ? &h->clock->done : nullptr;
         prof_begin(h, "stage");
         stage_kernel_mixed<<<g, STAGE_THREADS, 0, st>>>(a);
         prof_end(h);
@@ -803,6 +834,7 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
         h->cfl_nblocks = (long)sg.x * sg.y * sg.z;
     }
     bytes += 2 * (((size_t)h->cfl_nblocks * 8 + 255) / 256 * 256);  // stage CFL minima, kinetic energy
+    bytes += 256;                                              // device clock
     cudaError_t e = cudaMalloc(&h->pool, bytes);
     if (e != cudaSuccess) { delete h; cudaGetLastError(); return NS3D_ERR_OOM; }
     h->pool_bytes = bytes;
@@ -826,6 +858,8 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     h->cfl_part = (double *)p;
     p += ((size_t)h->cfl_nblocks * 8 + 255) / 256 * 256;
     h->ke_part = (double *)p;
+    p += ((size_t)h->cfl_nblocks * 8 + 255) / 256 * 256;
+    h->clock = (DevClock *)p;
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { cudaFree(h->pool); delete h; return NS3D_ERR_CUDA; }
     h->own_stream = true;
@@ -872,7 +906,8 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
 int ns3d_destroy(ns3d_handle *h) {
     if (!h) return NS3D_ERR_INVALID_ARG;
     cudaSetDevice(h->device);
-    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+    for (auto &g : h->adv_graph)
+        if (g) cudaGraphExecDestroy(g);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto &p : h->prof)
         for (auto e : p.ev) cudaEventDestroy(e);
@@ -896,7 +931,8 @@ int ns3d_set_stream(ns3d_handle *h, void *stream) {
     if (h->own_stream) cudaStreamDestroy(h->stream);
     if (stream) { h->stream = (cudaStream_t)stream; h->own_stream = false; }
     else { CK(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream"); h->own_stream = true; }
-    if (h->step_graph) { cudaGraphExecDestroy(h->step_graph); h->step_graph = nullptr; }
+    for (auto &g : h->adv_graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     return NS3D_OK;
 }
 
@@ -1246,9 +1282,101 @@ int ns3d_total_energy(ns3d_handle *h, double *ke_out) {
 }
 
 // time_advance's dt schedule (maincycle.cpp:18-56) without output.
+// Steps per captured time-advance graph: a multiple of 3, so the buffer
+// rotation of a full launch returns to where it started.
+constexpr int ADV_STEPS = 12;
+
+// The CFL minimum of the current state into clock->cfl_min: from the last
+// stage's per-block minima when they describe it, else the separate reduction.
+int seed_cfl_min(ns3d_handle *h) {
+    if (h->cfl_valid) {
+        min_combine_kernel<<<h->red_blocks, 256, 0, h->stream>>>(h->cfl_part, h->cfl_nblocks, h->partials);
+    } else if (!h->mixed) {
+        dt_kernel64<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
+                                                                  h->ph.dx, h->partials);
+    } else {
+        dt_kernel_mixed<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
+                                                                      h->ph.dx, h->partials);
+    }
+    min_combine_kernel<<<1, 256, 0, h->stream>>>(h->partials, h->red_blocks, &h->clock->cfl_min);
+    h->launches += 2;
+    CK(h, cudaGetLastError(), "cfl seed");
+    return NS3D_OK;
+}
+
+// Capture ADV_STEPS device-scheduled steps starting from buffer rotation s0:
+// schedule -> three (RHS, stage) pairs reading dt from the clock -> the CFL
+// minimum of the new state into the clock for the next step.
+int capture_adv_graph(ns3d_handle *h, int s0) {
+    // one ordinary RHS first: every kernel's attributes are set and its
+    // launch checked before any of it is captured (it only writes the RHS
+    // scratch arrays)
+    int rr = compute_rhs_async(h);
+    if (rr) return rr;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    const int keep = h->s0;
+    h->s0 = s0;
+    h->dev_loop = true;
+    cudaGraph_t g = nullptr;
+    int r = NS3D_OK;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        for (int n = 0; n < ADV_STEPS && r == NS3D_OK; ++n) {
+            schedule_kernel<<<1, 1, 0, h->stream>>>(h->clock, h->P.cfl, h->P.dt_fixed, 1e-12);
+            r = rk3_async(h, 0.0);
+            if (r == NS3D_OK) {
+                min_combine_kernel<<<h->red_blocks, 256, 0, h->stream>>>(h->cfl_part, h->cfl_nblocks, h->partials);
+                min_combine_kernel<<<1, 256, 0, h->stream>>>(h->partials, h->red_blocks, &h->clock->cfl_min);
+            }
+        }
+        cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+        if (e == cudaSuccess) e = e2;
+    }
+    h->dev_loop = false;
+    h->s0 = keep;
+    if (r == NS3D_OK && e == cudaSuccess) e = cudaGraphInstantiate(&h->adv_graph[s0], g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (r != NS3D_OK) return r;
+    if (e != cudaSuccess) { h->adv_graph[s0] = nullptr; return cuda_fail(h, e, "time-advance graph"); }
+    return NS3D_OK;
+}
+
+// time_advance with the dt schedule on the device: ADV_STEPS steps per graph
+// launch, one host synchronisation per launch.  Same dt sequence and state as
+// the host loop below, bit for bit.
+int time_advance_device(ns3d_handle *h, double t_end, int max_steps, double *time, int *steps_done) {
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    DevClock c{*time, 0.0, t_end, 0.0, 0, 0, max_steps, 0};
+    CK(h, cudaMemcpyAsync(h->clock, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream), "clock");
+    if (h->P.dt_fixed < 0.0 && (r = seed_cfl_min(h))) return r;
+    int total = 0;
+    while (true) {
+        const int s0 = h->s0;
+        if (!h->adv_graph[s0] && (r = capture_adv_graph(h, s0))) return r;
+        CK(h, cudaGraphLaunch(h->adv_graph[s0], h->stream), "graph launch");
+        h->launches += (long)ADV_STEPS * (3 + 3 * ((h->ph.mu != 0.0 ? 1 : 0) + 4));
+        CK(h, cudaMemcpyAsync(&c, h->clock, sizeof(c), cudaMemcpyDeviceToHost, h->stream), "clock");
+        CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+        const int ran = c.steps - total;  // steps this launch executed (the rest returned at once)
+        total = c.steps;
+        h->s0 = (s0 + ran) % 3;
+        if (ran > 0) h->cfl_valid = true;
+        if ((r = check_device_error(h))) break;
+        if (c.err) { r = fail(h, NS3D_ERR_DT, "dt too small or zero"); break; }
+        if (h->P.check_state && ran > 0 && (r = check_state(h))) break;
+        if (c.done) break;
+    }
+    *time = c.t;
+    if (steps_done) *steps_done = total;
+    return r;
+}
+
 int ns3d_time_advance(ns3d_handle *h, double t_end, int max_steps, double *time, int *steps_done) {
     if (!h || !time) return NS3D_ERR_INVALID_ARG;
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    // per-kernel event profiling cannot sit inside a captured graph
+    if (!h->profiling && max_steps > 0) return time_advance_device(h, t_end, max_steps, time, steps_done);
     const double eps = 1e-12;
     int done = 0, r = NS3D_OK;
     double t = *time;

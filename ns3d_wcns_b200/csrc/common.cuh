@@ -36,6 +36,14 @@ inline Layout make_layout(int nx, int ny, int nz) {
     return L;
 }
 
+// Device-resident time-advance state (the dt schedule of time_advance,
+// maincycle.cpp:18-56, run on the device so that many steps need no host
+// round trip).  While `done` is set every kernel of a step returns at once.
+struct DevClock {
+    double t, dt, t_end, cfl_min;
+    int done, steps, budget, err;
+};
+
 // Physical constants (initialization.cpp:194-197, field_structures.h:95).
 struct Phys {
     double gamma, Rgas, Cp, Pr, mu, S;

@@ -36,6 +36,8 @@ struct StageArgs64 {
     double *cfl_part;       // non-null: per-block minimum CFL bound of the new state
     double *ke_part;        // with cfl_part: per-block kinetic energy of the new state
     double dx, vol;
+    const double *dt_dev;   // non-null: dt from the device time loop (replaces dt)
+    const int *done;        // non-null: skip the launch while *done
 };
 
 constexpr int STAGE_THREADS = 128;
@@ -52,6 +54,8 @@ __device__ __forceinline__ void stage_partials(double *cfl_part, double *ke_part
 }
 
 __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel64(StageArgs64 a) {
+    if (a.done && *a.done) return;  // uniform over the grid
+    const double dt = a.dt_dev ? *a.dt_dev : a.dt;
     const Layout &L = a.L;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
@@ -84,7 +88,7 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel64(StageArgs64 a) {
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
                 const double r = inner ? a.Rhs[q][s] : 0.0;
-                Un[q] = rk_combine(a.stage, U0[q], U[q], r, a.dt);
+                Un[q] = rk_combine(a.stage, U0[q], U[q], r, dt);
             }
             c2p_exact(Un, a.gamma, W);
         }
@@ -124,9 +128,13 @@ struct StageArgsMixed {
     double *cfl_part;       // non-null: per-block minimum CFL bound of the new state
     double *ke_part;        // with cfl_part: per-block kinetic energy of the new state
     double dx, vol;
+    const double *dt_dev;   // non-null: dt from the device time loop (replaces dt)
+    const int *done;        // non-null: skip the launch while *done
 };
 
 __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel_mixed(StageArgsMixed a) {
+    if (a.done && *a.done) return;  // uniform over the grid
+    const double dt = a.dt_dev ? *a.dt_dev : a.dt;
     const Layout &L = a.L;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
@@ -154,9 +162,9 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel_mixed(StageArgsMix
                 const double r = inner ? (double)a.Rhs[q][s32] : 0.0;
                 const double u0 = a.U0[q][s];
                 const double u = a.stage == 1 ? u0 : a.Uc[q][s];
-                U[q] = a.stage == 1 ? u0 + a.dt * r
-                     : a.stage == 2 ? 0.75 * u0 + 0.25 * (u + a.dt * r)
-                                    : (1.0 / 3.0) * u0 + (2.0 / 3.0) * (u + a.dt * r);
+                U[q] = a.stage == 1 ? u0 + dt * r
+                     : a.stage == 2 ? 0.75 * u0 + 0.25 * (u + dt * r)
+                                    : (1.0 / 3.0) * u0 + (2.0 / 3.0) * (u + dt * r);
             }
         }
         if (U[0] <= 0.0) U[0] = 1e-12;

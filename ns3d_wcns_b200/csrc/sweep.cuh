@@ -47,6 +47,7 @@ struct SweepArgs {
     SchemeParams<R> sp;
     int first;          // 1: write (first direction), 0: accumulate
     int visc;           // 1: add the viscous divergence term
+    const int *done;    // non-null: skip the launch while *done (device time loop)
 };
 
 // Chunk geometry.  A chunk holds C faces of every line of the block.  Its
@@ -125,6 +126,7 @@ sweep_kernel(SweepArgs<R> a) {
     R *const stg = sW + (USE_W ? 5 * NL * NU : 0);   // [9][CH]
     R *const srold = stg + 9 * CH;                   // [5][CH] (kRoldSmem)
 
+    if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int line = DIR == 0 ? threadIdx.y : threadIdx.x;

@@ -36,6 +36,7 @@ struct ViscArgs {
     R dinv[3][3];           // per direction: 1/(2h), 1/(12h), 1/(60h)
     R mu0, S, cp_over_pr;
     int *err;               // device error word (a bounded wait that ran out)
+    const int *done;        // non-null: skip the launch while *done (device time loop)
 };
 
 // choose_scheme, ViscousFlux.cpp:33-50 (idx relative to the first interior node)
@@ -119,6 +120,7 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
     constexpr int TS = vtile_stride<R>();
     __shared__ __align__(128) R sm[2 * 4 * TS];  // two plane tiles of u, v, w, T
     __shared__ __align__(8) uint64_t bar[2];
+    if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
     const int x0 = blockIdx.x * VTX, y0 = blockIdx.y * VTY;
     const int kb = blockIdx.z * VZC, ke = min(kb + VZC, L.nz);

@@ -48,6 +48,7 @@ class Solver:
     def __init__(self, P: SolverParams, G: GridDesc, device: int = 0, check_state: bool = False):
         self.lib = _lib.load()
         self.P, self.G = P, G
+        self.device = device
         grid = _lib.Grid(G.global_nx, G.global_ny, G.global_nz, G.x0, G.y0, G.z0, G.Lx, G.Ly, G.Lz)
         h = C.c_void_p()
         r = self.lib.ns3d_create(C.byref(_params(P, device, check_state)), C.byref(grid), C.byref(h))
@@ -199,6 +200,40 @@ class Solver:
         lay = (C.c_long * 6)()
         self._check(self.lib.ns3d_device_fields(self.h, what, ptrs, lay))
         return [ptrs[i] for i in range(5)], list(lay)
+
+    def device_view(self, what: int):
+        """Zero-copy torch views (5, sz, sy, sx) of a device-resident group
+        (ghost-inclusive Field3D extents; the padding is skipped by strides)."""
+        import torch
+        ptrs, (sx, sy, sz, px, off, esz) = self.device_fields(what)
+        typestr = "<f8" if esz == 8 else "<f4"
+
+        class _Iface:
+            def __init__(self, ptr):
+                self.__cuda_array_interface__ = {
+                    "shape": (sz, sy, sx), "typestr": typestr, "data": (ptr + off * esz, False),
+                    "strides": (sy * px * esz, px * esz, esz), "version": 2}
+
+        return [torch.as_tensor(_Iface(p), device=f"cuda:{self.device}") for p in ptrs]
+
+    def turbulence_stats(self) -> Dict:
+        """Turbulence statistics of the current state computed on the GPU from
+        the resident fields (analysis.turbulence_stats: kinetic energy, u_rms,
+        nu, spectrum E(k) and dissipation 2 nu sum k^2 E(k), as the
+        reference's EnergySpectrum.cpp / ana_isotropic.cpp), FP64."""
+        from . import analysis
+        self.synchronize()
+        if int(self.P.precision) == int(Precision.MIXED):
+            rho, m1, m2, m3, E = (x[3:-3, 3:-3, 3:-3].double() for x in self.device_view(_lib.NS3D_CONSERVED))
+            u, v, w = m1 / rho, m2 / rho, m3 / rho
+            p = (self.P.gamma - 1.0) * (E - 0.5 * rho * (u * u + v * v + w * w))
+        else:
+            rho, u, v, w, p = (x[3:-3, 3:-3, 3:-3] for x in self.device_view(_lib.NS3D_PRIMITIVE))
+        Rgas = 1.0 / (self.P.gamma * self.P.Ma * self.P.Ma)
+        T = p / (rho * Rgas)
+        dV = (self.G.Lx / self.G.global_nx) * (self.G.Ly / self.G.global_ny) * (self.G.Lz / self.G.global_nz)
+        mu0 = 0.0 if self.P.Re == float("inf") else 1.0 / self.P.Re
+        return analysis.turbulence_stats(rho, u, v, w, T, mu0, self.P.S_ref, dV, device=f"cuda:{self.device}")
 
     def set_stream(self, stream_ptr: Optional[int]) -> None:
         self._check(self.lib.ns3d_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
