@@ -269,7 +269,7 @@ struct ns3d_handle {
     std::string err;
     DevClock *clock = nullptr;           // device time-advance state
     bool dev_loop = false;               // kernels being captured read dt / done from clock
-    cudaGraphExec_t adv_graph[3] = {};   // ADV_STEPS steps, per starting buffer rotation
+    cudaGraphExec_t adv_graph[3][3] = {};  // [length index][starting buffer rotation]
     double graph_dt = 0.0;
     int graph_s0 = -1;
     // per-kernel CUDA-event timing (ns3d_profile)
@@ -906,8 +906,9 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
 int ns3d_destroy(ns3d_handle *h) {
     if (!h) return NS3D_ERR_INVALID_ARG;
     cudaSetDevice(h->device);
-    for (auto &g : h->adv_graph)
-        if (g) cudaGraphExecDestroy(g);
+    for (auto &row : h->adv_graph)
+        for (auto &g : row)
+            if (g) cudaGraphExecDestroy(g);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto &p : h->prof)
         for (auto e : p.ev) cudaEventDestroy(e);
@@ -931,8 +932,9 @@ int ns3d_set_stream(ns3d_handle *h, void *stream) {
     if (h->own_stream) cudaStreamDestroy(h->stream);
     if (stream) { h->stream = (cudaStream_t)stream; h->own_stream = false; }
     else { CK(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream"); h->own_stream = true; }
-    for (auto &g : h->adv_graph)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (auto &row : h->adv_graph)
+        for (auto &g : row)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     return NS3D_OK;
 }
 
@@ -1282,9 +1284,11 @@ int ns3d_total_energy(ns3d_handle *h, double *ke_out) {
 }
 
 // time_advance's dt schedule (maincycle.cpp:18-56) without output.
-// Steps per captured time-advance graph: a multiple of 3, so the buffer
-// rotation of a full launch returns to where it started.
-constexpr int ADV_STEPS = 12;
+// Steps per captured time-advance graph.  A launch executes the longest
+// graph that fits the remaining step budget, so a budgeted run wastes no
+// launches; only the launch in which t_end is reached may carry steps that
+// return at once (a no-op step still costs about 0.1 ms of block scheduling).
+constexpr int ADV_LENS[3] = {12, 3, 1};
 
 // The CFL minimum of the current state into clock->cfl_min: from the last
 // stage's per-block minima when they describe it, else the separate reduction.
@@ -1304,10 +1308,10 @@ int seed_cfl_min(ns3d_handle *h) {
     return NS3D_OK;
 }
 
-// Capture ADV_STEPS device-scheduled steps starting from buffer rotation s0:
+// Capture ADV_LENS[li] device-scheduled steps starting from buffer rotation s0:
 // schedule -> three (RHS, stage) pairs reading dt from the clock -> the CFL
 // minimum of the new state into the clock for the next step.
-int capture_adv_graph(ns3d_handle *h, int s0) {
+int capture_adv_graph(ns3d_handle *h, int li, int s0) {
     // one ordinary RHS first: every kernel's attributes are set and its
     // launch checked before any of it is captured (it only writes the RHS
     // scratch arrays)
@@ -1315,13 +1319,14 @@ int capture_adv_graph(ns3d_handle *h, int s0) {
     if (rr) return rr;
     CK(h, cudaStreamSynchronize(h->stream), "synchronize");
     const int keep = h->s0;
+    const bool keep_valid = h->cfl_valid;  // capturing executes nothing: the stored minima stay as they were
     h->s0 = s0;
     h->dev_loop = true;
     cudaGraph_t g = nullptr;
     int r = NS3D_OK;
     cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        for (int n = 0; n < ADV_STEPS && r == NS3D_OK; ++n) {
+        for (int n = 0; n < ADV_LENS[li] && r == NS3D_OK; ++n) {
             schedule_kernel<<<1, 1, 0, h->stream>>>(h->clock, h->P.cfl, h->P.dt_fixed, 1e-12);
             r = rk3_async(h, 0.0);
             if (r == NS3D_OK) {
@@ -1334,28 +1339,35 @@ int capture_adv_graph(ns3d_handle *h, int s0) {
     }
     h->dev_loop = false;
     h->s0 = keep;
-    if (r == NS3D_OK && e == cudaSuccess) e = cudaGraphInstantiate(&h->adv_graph[s0], g, 0);
+    h->cfl_valid = keep_valid;
+    if (r == NS3D_OK && e == cudaSuccess) e = cudaGraphInstantiate(&h->adv_graph[li][s0], g, 0);
     if (g) cudaGraphDestroy(g);
     if (r != NS3D_OK) return r;
-    if (e != cudaSuccess) { h->adv_graph[s0] = nullptr; return cuda_fail(h, e, "time-advance graph"); }
+    if (e != cudaSuccess) { h->adv_graph[li][s0] = nullptr; return cuda_fail(h, e, "time-advance graph"); }
     return NS3D_OK;
 }
 
-// time_advance with the dt schedule on the device: ADV_STEPS steps per graph
+// time_advance with the dt schedule on the device: up to 12 steps per graph
 // launch, one host synchronisation per launch.  Same dt sequence and state as
 // the host loop below, bit for bit.
 int time_advance_device(ns3d_handle *h, double t_end, int max_steps, double *time, int *steps_done) {
     int r = set_device(h); if (r) return r;
     h->launches = 0;
+    // all graphs are captured at the first call of a handle, so no capture
+    // (and its set-up synchronisation) falls inside a later run
+    for (int li = 0; li < 3; ++li)
+        for (int b = 0; b < 3; ++b)
+            if (!h->adv_graph[li][b] && (r = capture_adv_graph(h, li, b))) return r;
     DevClock c{*time, 0.0, t_end, 0.0, 0, 0, max_steps, 0};
     CK(h, cudaMemcpyAsync(h->clock, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream), "clock");
     if (h->P.dt_fixed < 0.0 && (r = seed_cfl_min(h))) return r;
     int total = 0;
     while (true) {
         const int s0 = h->s0;
-        if (!h->adv_graph[s0] && (r = capture_adv_graph(h, s0))) return r;
-        CK(h, cudaGraphLaunch(h->adv_graph[s0], h->stream), "graph launch");
-        h->launches += (long)ADV_STEPS * (3 + 3 * ((h->ph.mu != 0.0 ? 1 : 0) + 4));
+        const int left = max_steps - total;
+        const int li = left >= ADV_LENS[0] ? 0 : (left >= ADV_LENS[1] ? 1 : 2);
+        CK(h, cudaGraphLaunch(h->adv_graph[li][s0], h->stream), "graph launch");
+        h->launches += (long)ADV_LENS[li] * (3 + 3 * ((h->ph.mu != 0.0 ? 1 : 0) + 4));
         CK(h, cudaMemcpyAsync(&c, h->clock, sizeof(c), cudaMemcpyDeviceToHost, h->stream), "clock");
         CK(h, cudaStreamSynchronize(h->stream), "synchronize");
         const int ran = c.steps - total;  // steps this launch executed (the rest returned at once)
