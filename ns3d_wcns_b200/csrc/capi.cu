@@ -260,7 +260,8 @@ struct ns3d_handle {
     CUtensorMap tmW64[3][3], tmT64, tmW32[3], tmT32;
     double *cfl_part = nullptr;   // per-block CFL minima written by the last RK stage
     double *ke_part = nullptr;    // per-block kinetic energy written by the last RK stage
-    long cfl_nblocks = 0;
+    long cfl_nblocks = 0;         // capacity of cfl_part / ke_part
+    long cfl_count = 0;           // partials the last stage-3 launch wrote
     bool cfl_valid = false;       // cfl_part describes the current state
     double *scalars = nullptr;
     int red_blocks = 0;
@@ -363,6 +364,7 @@ SweepArgs<R> sweep_args(ns3d_handle *h, int dir) {
     static const int comp[3][4] = {{0, 3, 4, 6}, {3, 1, 5, 7}, {4, 5, 2, 8}};
     for (int q = 0; q < 4; ++q) a.V[q] = (const R *)h->visc[comp[dir][q]];
     a.done = h->dev_loop ? &h->clock->done : nullptr;
+    a.fs = FusedStage{};  // stage 0: the sweep writes the right-hand side
     return a;
 }
 
@@ -423,7 +425,7 @@ ViscArgs<R> visc_args(ns3d_handle *h) {
 }
 
 template <typename R>
-int rhs_impl(ns3d_handle *h) {
+int rhs_impl(ns3d_handle *h, const FusedStage *fs = nullptr) {
     cudaStream_t st = h->stream;
     cudaError_t e;
     if (h->ph.mu != 0.0) {  // Re = inf: the viscous terms are exactly zero
@@ -444,8 +446,10 @@ int rhs_impl(ns3d_handle *h) {
     prof_begin(h, "sweep_y");
     e = sweep_y(sweep_args<R>(h, 1), st); if (e != cudaSuccess) return cuda_fail(h, e, "sweep_y");
     prof_end(h);
-    prof_begin(h, "sweep_z");
-    e = sweep_z(sweep_args<R>(h, 2), st); if (e != cudaSuccess) return cuda_fail(h, e, "sweep_z");
+    SweepArgs<R> az = sweep_args<R>(h, 2);
+    if (fs) az.fs = *fs;
+    prof_begin(h, fs ? "sweep_z_stage" : "sweep_z");
+    e = sweep_z(az, st); if (e != cudaSuccess) return cuda_fail(h, e, "sweep_z");
     prof_end(h);
     h->launches += 3;
     return NS3D_OK;
@@ -494,6 +498,56 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
     h->cfl_valid = false;
     CK(h, cudaGetLastError(), "stage kernel");
     h->cfl_valid = stage == 3;
+    if (stage == 3) h->cfl_count = (long)g.x * g.y * g.z;
+    return NS3D_OK;
+}
+
+// One RK stage: right-hand side and update.  Plain FP64 path: the update is
+// fused into the z-sweep (FusedStage) and a ghost kernel fills the ghost cells
+// -- the same bits as the separate stage kernel; mixed path: RHS then the
+// separate stage kernel.  src0 = step-start state, srcc = this stage's state
+// (the sweeps read h->s0, which the caller has set to srcc), dst = new state.
+int rk_stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double dt) {
+    if (h->mixed) {
+        // the mixed path keeps the separate stage kernel: fused into the FP32
+        // z-sweep its FP64 conversions cost more than the pass they save
+        int r = compute_rhs_async(h);
+        if (r) return r;
+        return stage_async(h, stage, src0, srcc, dst, dt);
+    }
+    FusedStage f{};
+    f.stage = stage;
+    for (int q = 0; q < 5; ++q) { f.W0[q] = h->S[src0][q]; f.Wout[q] = h->S[dst][q]; }
+    f.Tout = h->T64;
+    f.dt = dt;
+    f.dt_dev = h->dev_loop ? &h->clock->dt : nullptr;
+    f.gamma = h->ph.gamma; f.Rgas = h->ph.Rgas; f.dx = h->ph.dx;
+    f.vol = h->ph.dx * h->ph.dy * h->ph.dz;
+    f.cfl_part = stage == 3 ? h->cfl_part : nullptr;
+    f.ke_part = stage == 3 ? h->ke_part : nullptr;
+    h->cfl_valid = false;
+    int r = rhs_impl<double>(h, &f);
+    if (r) return r;
+    StageArgs64 a;
+    for (int q = 0; q < 5; ++q) {
+        a.W0[q] = h->S[src0][q]; a.Wc[q] = h->S[srcc][q]; a.Rhs[q] = h->rhs64[q]; a.Wout[q] = h->S[dst][q];
+    }
+    a.L = h->L64; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
+    a.Tout = h->T64; a.Rgas = h->ph.Rgas;
+    a.cfl_part = nullptr; a.ke_part = nullptr; a.dx = h->ph.dx; a.vol = f.vol;
+    a.dt_dev = f.dt_dev;
+    a.done = h->dev_loop ? &h->clock->done : nullptr;
+    const long ng = ghost_count(h->L64);
+    prof_begin(h, "ghost_fill");
+    stage_ghost_kernel64<<<(unsigned)((ng + 255) / 256), 256, 0, h->stream>>>(a);
+    prof_end(h);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "ghost kernel");
+    if (stage == 3) {
+        const int gx = (h->L64.nx + SweepGeom<2>::NLINE - 1) / SweepGeom<2>::NLINE;
+        h->cfl_count = (long)gx * h->L64.ny;  // z-sweep blocks
+        h->cfl_valid = true;
+    }
     return NS3D_OK;
 }
 
@@ -502,15 +556,16 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
 // the pointer rotation).
 int rk3_async(ns3d_handle *h, double dt) {
     const int s0 = h->s0, b1 = (s0 + 1) % 3, b2 = (s0 + 2) % 3;
+    auto fail_reset = [&](int r) {  // back to the step's start buffer
+        h->s0 = s0;
+        return r;
+    };
     int r;
-    if ((r = compute_rhs_async(h)) != NS3D_OK) return r;
-    if ((r = stage_async(h, 1, s0, s0, b1, dt)) != NS3D_OK) return r;
+    if ((r = rk_stage_async(h, 1, s0, s0, b1, dt)) != NS3D_OK) return fail_reset(r);
     h->s0 = b1;  // RHS of stage 2 reads the stage-1 state
-    if ((r = compute_rhs_async(h)) != NS3D_OK) { h->s0 = s0; return r; }
-    if ((r = stage_async(h, 2, s0, b1, b2, dt)) != NS3D_OK) { h->s0 = s0; return r; }
+    if ((r = rk_stage_async(h, 2, s0, b1, b2, dt)) != NS3D_OK) return fail_reset(r);
     h->s0 = b2;
-    if ((r = compute_rhs_async(h)) != NS3D_OK) { h->s0 = s0; return r; }
-    if ((r = stage_async(h, 3, s0, b2, b1, dt)) != NS3D_OK) { h->s0 = s0; return r; }
+    if ((r = rk_stage_async(h, 3, s0, b2, b1, dt)) != NS3D_OK) return fail_reset(r);
     h->s0 = b1;
     return NS3D_OK;
 }
@@ -661,16 +716,13 @@ int rk3_async_store(ns3d_handle *h, double dt, double *const st[3][5]) {
     const int s0 = h->s0, b1 = (s0 + 1) % 3, b2 = (s0 + 2) % 3;
     int r;
     for (int q = 0; q < 5; ++q) CK(h, cudaMemcpyAsync(st[0][q], h->S[s0][q], bytes, cudaMemcpyDeviceToDevice, h->stream), "store");
-    if ((r = compute_rhs_async(h))) return r;
-    if ((r = stage_async(h, 1, s0, s0, b1, dt))) return r;
+    if ((r = rk_stage_async(h, 1, s0, s0, b1, dt))) return r;
     for (int q = 0; q < 5; ++q) CK(h, cudaMemcpyAsync(st[1][q], h->S[b1][q], bytes, cudaMemcpyDeviceToDevice, h->stream), "store");
     h->s0 = b1;
-    if ((r = compute_rhs_async(h))) { h->s0 = s0; return r; }
-    if ((r = stage_async(h, 2, s0, b1, b2, dt))) { h->s0 = s0; return r; }
+    if ((r = rk_stage_async(h, 2, s0, b1, b2, dt))) { h->s0 = s0; return r; }
     for (int q = 0; q < 5; ++q) CK(h, cudaMemcpyAsync(st[2][q], h->S[b2][q], bytes, cudaMemcpyDeviceToDevice, h->stream), "store");
     h->s0 = b2;
-    if ((r = compute_rhs_async(h))) { h->s0 = s0; return r; }
-    if ((r = stage_async(h, 3, s0, b2, b1, dt))) { h->s0 = s0; return r; }
+    if ((r = rk_stage_async(h, 3, s0, b2, b1, dt))) { h->s0 = s0; return r; }
     h->s0 = b1;
     return NS3D_OK;
 }
@@ -1194,7 +1246,7 @@ int ns3d_compute_timestep(ns3d_handle *h, double *dt_out) {
         // the last RK stage left the per-block minima of this state
         prof_begin(h, "cfl_combine");
         const int nb = h->red_blocks;  // partials holds at least red_blocks values
-        min_combine_kernel<<<nb, 256, 0, h->stream>>>(h->cfl_part, h->cfl_nblocks, h->partials);
+        min_combine_kernel<<<nb, 256, 0, h->stream>>>(h->cfl_part, h->cfl_count, h->partials);
         min_combine_kernel<<<1, 256, 0, h->stream>>>(h->partials, nb, h->scalars);
         prof_end(h);
         h->launches += 2;
@@ -1268,7 +1320,7 @@ int ns3d_total_energy(ns3d_handle *h, double *ke_out) {
         int r = set_device(h); if (r) return r;
         h->launches = 0;
         const int nb = h->red_blocks;
-        sum_combine_kernel<<<nb, 256, 0, h->stream>>>(h->ke_part, h->cfl_nblocks, h->partials);
+        sum_combine_kernel<<<nb, 256, 0, h->stream>>>(h->ke_part, h->cfl_count, h->partials);
         sum_combine_kernel<<<1, 256, 0, h->stream>>>(h->partials, nb, h->scalars);
         h->launches += 2;
         CK(h, cudaGetLastError(), "kinetic energy combine");
@@ -1294,7 +1346,7 @@ constexpr int ADV_LENS[3] = {12, 3, 1};
 // stage's per-block minima when they describe it, else the separate reduction.
 int seed_cfl_min(ns3d_handle *h) {
     if (h->cfl_valid) {
-        min_combine_kernel<<<h->red_blocks, 256, 0, h->stream>>>(h->cfl_part, h->cfl_nblocks, h->partials);
+        min_combine_kernel<<<h->red_blocks, 256, 0, h->stream>>>(h->cfl_part, h->cfl_count, h->partials);
     } else if (!h->mixed) {
         dt_kernel64<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
                                                                   h->ph.dx, h->partials);
@@ -1330,7 +1382,7 @@ int capture_adv_graph(ns3d_handle *h, int li, int s0) {
             schedule_kernel<<<1, 1, 0, h->stream>>>(h->clock, h->P.cfl, h->P.dt_fixed, 1e-12);
             r = rk3_async(h, 0.0);
             if (r == NS3D_OK) {
-                min_combine_kernel<<<h->red_blocks, 256, 0, h->stream>>>(h->cfl_part, h->cfl_nblocks, h->partials);
+                min_combine_kernel<<<h->red_blocks, 256, 0, h->stream>>>(h->cfl_part, h->cfl_count, h->partials);
                 min_combine_kernel<<<1, 256, 0, h->stream>>>(h->partials, h->red_blocks, &h->clock->cfl_min);
             }
         }

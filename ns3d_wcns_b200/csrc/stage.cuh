@@ -191,4 +191,125 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel_mixed(StageArgsMix
     if (a.cfl_part) stage_partials(a.cfl_part, a.ke_part, cfl, ke);
 }
 
+// ----------------------------------------------------- ghost fill after a fused stage
+
+// Ghost cells only, one thread each: t enumerates the two z-slabs (full x-y
+// planes), then the y-slabs of the interior planes, then the x-ghosts of the
+// interior rows.
+__device__ __forceinline__ bool ghost_cell(const Layout &L, long t, int &i, int &j, int &k) {
+    const long gz = 6L * L.sy * L.sx, gy = 6L * L.nz * L.sx, gx = 6L * L.nz * L.ny;
+    if (t < gz) {
+        const long sl = t / ((long)L.sy * L.sx), rem = t % ((long)L.sy * L.sx);
+        k = sl < 3 ? (int)sl : L.nz + (int)sl; j = (int)(rem / L.sx); i = (int)(rem % L.sx);
+        return true;
+    }
+    t -= gz;
+    if (t < gy) {
+        k = (int)(t / (6L * L.sx)) + NG;
+        const long rem = t % (6L * L.sx), sl = rem / L.sx;
+        j = sl < 3 ? (int)sl : L.ny + (int)sl; i = (int)(rem % L.sx);
+        return true;
+    }
+    t -= gy;
+    if (t < gx) {
+        const long row = t / 6, sl = t % 6;
+        k = (int)(row / L.ny) + NG; j = (int)(row % L.ny) + NG;
+        i = sl < 3 ? (int)sl : L.nx + (int)sl;
+        return true;
+    }
+    return false;
+}
+
+__host__ __device__ inline long ghost_count(const Layout &L) {
+    return 6L * L.sy * L.sx + 6L * L.nz * L.sx + 6L * L.nz * L.ny;
+}
+
+// After the z-sweep wrote the new interior state (fused stage), the ghost
+// cells receive exactly what stage_kernel64 gives them: a copy (with sign
+// flips) of their source's new value when the source is interior, the stage
+// combination with a zero right-hand side when it is a ghost, or a constant.
+__global__ void __launch_bounds__(256) stage_ghost_kernel64(StageArgs64 a) {
+    if (a.done && *a.done) return;
+    const Layout &L = a.L;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!ghost_cell(L, t, i, j, k)) return;
+    const double dt = a.dt_dev ? *a.dt_dev : a.dt;
+    int c[3] = {i, j, k};
+    int flip;
+    const int kind = resolve_source(L, a.b, c, flip);
+    double W[5];
+    if (kind != SRC_CELL) {
+        special_state(kind, W);
+    } else {
+        const long s = L.at(c[0], c[1], c[2]);
+        if (is_interior(L, c)) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) W[q] = a.Wout[q][s];
+        } else {
+            double U0[5], U[5], Un[5];
+            p2c_exact(a.W0[0][s], a.W0[1][s], a.W0[2][s], a.W0[3][s], a.W0[4][s], a.gamma, U0);
+            if (a.stage == 1) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) U[q] = U0[q];
+            } else {
+                p2c_exact(a.Wc[0][s], a.Wc[1][s], a.Wc[2][s], a.Wc[3][s], a.Wc[4][s], a.gamma, U);
+            }
+#pragma unroll
+            for (int q = 0; q < 5; ++q) Un[q] = rk_combine(a.stage, U0[q], U[q], 0.0, dt);
+            c2p_exact(Un, a.gamma, W);
+        }
+    }
+    apply_flips(flip, W);
+    const long o = L.at(i, j, k);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) a.Wout[q][o] = W[q];
+    a.Tout[o] = W[4] / __dmul_rn(W[0], a.Rgas);
+}
+
+__global__ void __launch_bounds__(256) stage_ghost_kernel_mixed(StageArgsMixed a) {
+    if (a.done && *a.done) return;
+    const Layout &L = a.L;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!ghost_cell(L, t, i, j, k)) return;
+    const double dt = a.dt_dev ? *a.dt_dev : a.dt;
+    int c[3] = {i, j, k};
+    int flip;
+    const int kind = resolve_source(L, a.b, c, flip);
+    double U[5], W[5];
+    if (kind != SRC_CELL) {
+        special_state(kind, W);
+        apply_flips(flip, W);
+        p2c_exact(W[0], W[1], W[2], W[3], W[4], a.gamma, U);
+    } else {
+        const long s = L.at(c[0], c[1], c[2]);
+        if (is_interior(L, c)) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) U[q] = a.Uout[q][s];  // new value, already clamped
+        } else {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const double u0 = a.U0[q][s];
+                const double u = a.stage == 1 ? u0 : a.Uc[q][s];
+                U[q] = a.stage == 1 ? u0 + dt * 0.0
+                     : a.stage == 2 ? 0.75 * u0 + 0.25 * (u + dt * 0.0)
+                                    : (1.0 / 3.0) * u0 + (2.0 / 3.0) * (u + dt * 0.0);
+            }
+            if (U[0] <= 0.0) U[0] = 1e-12;
+        }
+        if (flip & 1) U[1] = -U[1];
+        if (flip & 2) U[2] = -U[2];
+        if (flip & 4) U[3] = -U[3];
+        c2p_exact(U, a.gamma, W);
+    }
+    const long o = L.at(i, j, k);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) a.Uout[q][o] = U[q];
+    const long o32 = a.L32.at(i, j, k);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) a.Wout[q][o32] = (float)W[q];
+    a.Tout[o32] = (float)(W[4] / (W[0] * a.Rgas));
+}
+
 }  // namespace ns3d

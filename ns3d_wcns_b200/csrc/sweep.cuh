@@ -27,11 +27,33 @@
 // x-lines and the warps march.
 #pragma once
 
+#include "bc.cuh"
 #include "common.cuh"
+#include "reduce.cuh"
 #include "schemes.cuh"
 #include "viscous.cuh"
 
 namespace ns3d {
+
+// The RK stage fused into the last (z) sweep of the plain FP64 path: for every
+// interior cell the sweep holds the final right-hand side in registers and
+// the current conserved state in its shared buffer, so it applies
+// runge_kutta_3's update and conversion (range_kutta.cpp:53-91) itself and
+// writes the new primitives instead of the right-hand side; a ghost kernel
+// then fills the ghost cells.  stage 0: no fusion (the sweep writes the
+// right-hand side).  (The mixed path keeps its separate stage kernel: there the
+// FP64 conversions would run at the FP32 sweep's occupancy and cost more than
+// the pass they save.)
+struct FusedStage {
+    int stage;
+    const double *W0[5];    // step-start primitives
+    double *Wout[5];        // new primitives
+    double *Tout;
+    double dt;
+    const double *dt_dev;   // non-null: dt from the device time loop
+    double gamma, Rgas, dx, vol;
+    double *cfl_part, *ke_part;  // stage 3: per-block CFL minimum and kinetic energy
+};
 
 template <typename R>
 struct SweepArgs {
@@ -48,6 +70,7 @@ struct SweepArgs {
     int first;          // 1: write (first direction), 0: accumulate
     int visc;           // 1: add the viscous divergence term
     const int *done;    // non-null: skip the launch while *done (device time loop)
+    FusedStage fs;      // z-sweep only
 };
 
 // Chunk geometry.  A chunk holds C faces of every line of the block.  Its
@@ -112,6 +135,27 @@ __device__ __forceinline__ R dstencil_inv(F f, int order, const R *dinv) {
     return (-f(2) + R(8) * f(1) - R(8) * f(-1) + f(-2)) * dinv[1];
 }
 
+// Stage update of interior cell c (padded FP64 index) from its final
+// right-hand side r and current conserved state Uc (the sweep's exact p2c of
+// W): the operations of stage_kernel64 for an interior cell, so the same bits.
+__device__ __forceinline__ void fused_stage_cell(const FusedStage &f, double dt, long c, const double *r,
+                                                 const double *Ucur, double &cfl, double &ke) {
+    double U0[5], U[5], W[5];
+    p2c_exact(f.W0[0][c], f.W0[1][c], f.W0[2][c], f.W0[3][c], f.W0[4][c], f.gamma, U0);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) U[q] = rk_combine(f.stage, U0[q], f.stage == 1 ? U0[q] : Ucur[q], r[q], dt);
+    c2p_exact(U, f.gamma, W);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) f.Wout[q][c] = W[q];
+    f.Tout[c] = W[4] / __dmul_rn(W[0], f.Rgas);
+    if (f.stage == 3) {
+        double Un[5];
+        p2c_exact(W[0], W[1], W[2], W[3], W[4], f.gamma, Un);
+        cfl = fmin(cfl, cfl_bound(Un, f.gamma, f.dx));
+        ke += 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * f.vol;
+    }
+}
+
 template <int DIR, typename R, int INTERP, int RS, int CHAR>
 __global__ void __launch_bounds__(256, sweep_min_blocks<R>())
 sweep_kernel(SweepArgs<R> a) {
@@ -128,6 +172,9 @@ sweep_kernel(SweepArgs<R> a) {
 
     if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
+    // fused stage (FP64 z-sweep): dt, and the thread's CFL minimum / kinetic energy
+    const double fdt = (DIR == 2 && sizeof(R) == 8 && a.fs.stage) ? (a.fs.dt_dev ? *a.fs.dt_dev : a.fs.dt) : 0.0;
+    double cfl_acc = 1e9, ke_acc = 0.0;  // 1e9: the initial minimum of the CFL reductions
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int line = DIR == 0 ? threadIdx.y : threadIdx.x;
     const int ta0 = blockIdx.x * NL + line, tb0 = blockIdx.y;
@@ -364,11 +411,28 @@ sweep_kernel(SweepArgs<R> a) {
                             o, a.dinv);
                 }
             }
+            R rq[5];
 #pragma unroll
             for (int q = 0; q < 5; ++q) {
-                R r = rold[q] - d[q];
-                if (q > 0) r += vd[q - 1];
-                a.Rhs[q][cid] = r;
+                rq[q] = rold[q] - d[q];
+                if (q > 0) rq[q] += vd[q - 1];
+            }
+            bool fused = false;
+            if constexpr (DIR == 2 && sizeof(R) == 8) {
+                if (a.fs.stage) {
+                    double Uc[5], rr[5];
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) {
+                        Uc[q] = sU[q * NL * NU + G::template idx<NU>(line, slot)];
+                        rr[q] = rq[q];
+                    }
+                    fused_stage_cell(a.fs, fdt, cid, rr, Uc, cfl_acc, ke_acc);
+                    fused = true;
+                }
+            }
+            if (!fused) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) a.Rhs[q][cid] = rq[q];
             }
         }
         cp_async_wait<0>();
@@ -405,6 +469,9 @@ sweep_kernel(SweepArgs<R> a) {
             }
         }
     }
+    if (DIR == 2 && sizeof(R) == 8 && a.fs.stage == 3)  // uniform: every thread of the block arrives
+        block_min_sum_n<CH>(cfl_acc, ke_acc, a.fs.cfl_part + (long)blockIdx.y * gridDim.x + blockIdx.x,
+                            a.fs.ke_part + (long)blockIdx.y * gridDim.x + blockIdx.x);
 }
 
 template <int DIR, typename R, int INTERP, int RS, int CHAR>
