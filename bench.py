@@ -544,7 +544,10 @@ def main():
                  "kernels_ms": {k: round(v["ms"] / max(v["launches"], 1), 4) for k, v in (profm or {}).items()}}
 
     # roofline of the dominant kernel (algorithmic bytes per launch / event time)
-    algo_bytes_per_cell = {"sweep_x": 80, "sweep_y": 120, "sweep_z": 120, "viscous_flux": 40 + 72,
+    # sweep_z_stage (FP64: z-sweep with the RK update fused in): z-sweep 120 + stage 160
+    # of the per-kernel figures, less the RHS write, its re-read and the stage's state read
+    algo_bytes_per_cell = {"sweep_x": 80, "sweep_y": 120, "sweep_z": 120, "sweep_z_stage": 160,
+                           "viscous_flux": 40 + 72,
                            "viscous_div": 72 + 64, "stage": 160, "cfl_dt": 40}
     dom = max(prof, key=lambda k: prof[k]["ms"])
     avg_ms = prof[dom]["ms"] / prof[dom]["launches"]

@@ -139,7 +139,7 @@ __device__ __forceinline__ R dstencil_inv(F f, int order, const R *dinv) {
 // right-hand side r and current conserved state Uc (the sweep's exact p2c of
 // W): the operations of stage_kernel64 for an interior cell, so the same bits.
 __device__ __forceinline__ void fused_stage_cell(const FusedStage &f, double dt, long c, const double *r,
-                                                 const double *Ucur, double &cfl, double &ke) {
+                                                 const double *Ucur, double &cfl, double &ke, double &kc) {
     double U0[5], U[5], W[5];
     p2c_exact(f.W0[0][c], f.W0[1][c], f.W0[2][c], f.W0[3][c], f.W0[4][c], f.gamma, U0);
 #pragma unroll
@@ -152,7 +152,12 @@ __device__ __forceinline__ void fused_stage_cell(const FusedStage &f, double dt,
         double Un[5];
         p2c_exact(W[0], W[1], W[2], W[3], W[4], f.gamma, Un);
         cfl = fmin(cfl, cfl_bound(Un, f.gamma, f.dx));
-        ke += 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * f.vol;
+        // a thread adds one cell per chunk along its line: compensated
+        // (Kahan) summation keeps its partial exact to rounding
+        const double y = 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * f.vol - kc;
+        const double t = __dadd_rn(ke, y);
+        kc = __dsub_rn(__dsub_rn(t, ke), y);
+        ke = t;
     }
 }
 
@@ -174,7 +179,7 @@ sweep_kernel(SweepArgs<R> a) {
     const Layout &L = a.L;
     // fused stage (FP64 z-sweep): dt, and the thread's CFL minimum / kinetic energy
     const double fdt = (DIR == 2 && sizeof(R) == 8 && a.fs.stage) ? (a.fs.dt_dev ? *a.fs.dt_dev : a.fs.dt) : 0.0;
-    double cfl_acc = 1e9, ke_acc = 0.0;  // 1e9: the initial minimum of the CFL reductions
+    double cfl_acc = 1e9, ke_acc = 0.0, ke_c = 0.0;  // 1e9: the initial minimum of the CFL reductions
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int line = DIR == 0 ? threadIdx.y : threadIdx.x;
     const int ta0 = blockIdx.x * NL + line, tb0 = blockIdx.y;
@@ -426,7 +431,7 @@ sweep_kernel(SweepArgs<R> a) {
                         Uc[q] = sU[q * NL * NU + G::template idx<NU>(line, slot)];
                         rr[q] = rq[q];
                     }
-                    fused_stage_cell(a.fs, fdt, cid, rr, Uc, cfl_acc, ke_acc);
+                    fused_stage_cell(a.fs, fdt, cid, rr, Uc, cfl_acc, ke_acc, ke_c);
                     fused = true;
                 }
             }
@@ -470,7 +475,7 @@ sweep_kernel(SweepArgs<R> a) {
         }
     }
     if (DIR == 2 && sizeof(R) == 8 && a.fs.stage == 3)  // uniform: every thread of the block arrives
-        block_min_sum_n<CH>(cfl_acc, ke_acc, a.fs.cfl_part + (long)blockIdx.y * gridDim.x + blockIdx.x,
+        block_min_sum_n<CH>(cfl_acc, ke_acc - ke_c, a.fs.cfl_part + (long)blockIdx.y * gridDim.x + blockIdx.x,
                             a.fs.ke_part + (long)blockIdx.y * gridDim.x + blockIdx.x);
 }
 
