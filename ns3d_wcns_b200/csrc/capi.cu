@@ -509,16 +509,51 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
 // (the sweeps read h->s0, which the caller has set to srcc), dst = new state.
 int rk_stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double dt) {
     if (h->mixed) {
-        // the mixed path keeps the separate stage kernel: fused into the FP32
-        // z-sweep its FP64 conversions cost more than the pass they save
-        int r = compute_rhs_async(h);
+        FusedStage f{};
+        f.stage = stage;
+        for (int q = 0; q < 5; ++q) {
+            f.U0[q] = h->S[src0][q]; f.Uc[q] = h->S[srcc][q]; f.Uout[q] = h->S[dst][q];
+            f.W32out[q] = h->w32[q];  // in place (the sweep defers the cells its wrap re-reads)
+        }
+        f.T32out = h->T32;
+        f.L64 = h->L64;
+        f.dt = dt;
+        f.dt_dev = h->dev_loop ? &h->clock->dt : nullptr;
+        f.gamma = h->ph.gamma; f.Rgas = h->ph.Rgas; f.dx = h->ph.dx;
+        f.vol = h->ph.dx * h->ph.dy * h->ph.dz;
+        f.cfl_part = stage == 3 ? h->cfl_part : nullptr;
+        f.ke_part = stage == 3 ? h->ke_part : nullptr;
+        h->cfl_valid = false;
+        int r = rhs_impl<float>(h, &f);
         if (r) return r;
-        return stage_async(h, stage, src0, srcc, dst, dt);
+        StageArgsMixed a;
+        for (int q = 0; q < 5; ++q) {
+            a.U0[q] = h->S[src0][q]; a.Uc[q] = h->S[srcc][q]; a.Rhs[q] = h->rhs32[q];
+            a.Uout[q] = h->S[dst][q]; a.Wout[q] = h->w32[q];
+        }
+        a.L = h->L64; a.L32 = h->L32; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
+        a.Tout = h->T32; a.Rgas = h->ph.Rgas;
+        a.cfl_part = nullptr; a.ke_part = nullptr; a.dx = h->ph.dx; a.vol = f.vol;
+        a.dt_dev = f.dt_dev;
+        a.done = h->dev_loop ? &h->clock->done : nullptr;
+        const long ng = ghost_count(h->L64);
+        prof_begin(h, "ghost_fill");
+        stage_ghost_kernel_mixed<<<(unsigned)((ng + 255) / 256), 256, 0, h->stream>>>(a);
+        prof_end(h);
+        h->launches += 1;
+        CK(h, cudaGetLastError(), "ghost kernel");
+        if (stage == 3) {
+            const int gx = (h->L32.nx + SweepGeom<2>::NLINE - 1) / SweepGeom<2>::NLINE;
+            h->cfl_count = (long)gx * h->L32.ny;  // z-sweep blocks
+            h->cfl_valid = true;
+        }
+        return NS3D_OK;
     }
     FusedStage f{};
     f.stage = stage;
     for (int q = 0; q < 5; ++q) { f.W0[q] = h->S[src0][q]; f.Wout[q] = h->S[dst][q]; }
     f.Tout = h->T64;
+    f.L64 = h->L64;
     f.dt = dt;
     f.dt_dev = h->dev_loop ? &h->clock->dt : nullptr;
     f.gamma = h->ph.gamma; f.Rgas = h->ph.Rgas; f.dx = h->ph.dx;

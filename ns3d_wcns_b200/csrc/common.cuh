@@ -81,6 +81,18 @@ __device__ __forceinline__ void c2p_exact(const double U[5], double gamma, doubl
     W[4] = __dmul_rn(__dmul_rn(gamma - 1.0, rr), e);
 }
 
+// Mixed path: conserved -> primitive in FP64 with one reciprocal (the mixed
+// path has an accuracy bound, not a bitwise contract); the pressure
+// recovery p = (gamma-1)(E - rho |u|^2 / 2), which cancels at low Mach, stays
+// FP64.  Density clamp as field_structures.h:444-465.
+__device__ __forceinline__ void c2p_fast(const double U[5], double gamma, double W[5], double &irho) {
+    const double rr = U[0] <= 0.0 ? 1e-12 : U[0];
+    irho = 1.0 / rr;
+    const double u = U[1] * irho, v = U[2] * irho, w = U[3] * irho;
+    W[0] = rr; W[1] = u; W[2] = v; W[3] = w;
+    W[4] = (gamma - 1.0) * (U[4] - 0.5 * rr * (u * u + v * v + w * w));
+}
+
 // Float versions for the mixed path (no parity contract).
 __device__ __forceinline__ void p2c_f(float r, float u, float v, float w, float p, float gm1,
                                       float U[5]) {

@@ -277,11 +277,12 @@ __global__ void __launch_bounds__(256) stage_ghost_kernel_mixed(StageArgsMixed a
     int c[3] = {i, j, k};
     int flip;
     const int kind = resolve_source(L, a.b, c, flip);
-    double U[5], W[5];
+    double U[5], W[5], ir;
     if (kind != SRC_CELL) {
         special_state(kind, W);
         apply_flips(flip, W);
         p2c_exact(W[0], W[1], W[2], W[3], W[4], a.gamma, U);
+        ir = 1.0 / W[0];
     } else {
         const long s = L.at(c[0], c[1], c[2]);
         if (is_interior(L, c)) {
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(256) stage_ghost_kernel_mixed(StageArgsMixed a
         if (flip & 1) U[1] = -U[1];
         if (flip & 2) U[2] = -U[2];
         if (flip & 4) U[3] = -U[3];
-        c2p_exact(U, a.gamma, W);
+        c2p_fast(U, a.gamma, W, ir);  // the conversion the fused z-sweep gives the interior cells
     }
     const long o = L.at(i, j, k);
 #pragma unroll
@@ -309,7 +310,7 @@ __global__ void __launch_bounds__(256) stage_ghost_kernel_mixed(StageArgsMixed a
     const long o32 = a.L32.at(i, j, k);
 #pragma unroll
     for (int q = 0; q < 5; ++q) a.Wout[q][o32] = (float)W[q];
-    a.Tout[o32] = (float)(W[4] / (W[0] * a.Rgas));
+    a.Tout[o32] = (float)(W[4] * ir / a.Rgas);
 }
 
 }  // namespace ns3d

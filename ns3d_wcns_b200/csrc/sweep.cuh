@@ -35,20 +35,29 @@
 
 namespace ns3d {
 
-// The RK stage fused into the last (z) sweep of the plain FP64 path: for every
-// interior cell the sweep holds the final right-hand side in registers and
-// the current conserved state in its shared buffer, so it applies
-// runge_kutta_3's update and conversion (range_kutta.cpp:53-91) itself and
-// writes the new primitives instead of the right-hand side; a ghost kernel
-// then fills the ghost cells.  stage 0: no fusion (the sweep writes the
-// right-hand side).  (The mixed path keeps its separate stage kernel: there the
-// FP64 conversions would run at the FP32 sweep's occupancy and cost more than
-// the pass they save.)
+// The RK stage fused into the last (z) sweep: for every interior cell the
+// sweep holds the final right-hand side in registers and the current state,
+// so it applies runge_kutta_3's update (range_kutta.cpp:53-91) itself and
+// writes the new state instead of the right-hand side; a ghost kernel then
+// fills the ghost cells.  stage 0: no fusion (the sweep writes the RHS).
+//   plain FP64 path: W0 -> Wout, Tout; the current conserved state is the
+//     sweep's exact p2c of W (shared buffer), so the bits equal the separate
+//     stage kernel's;
+//   mixed path: FP64 conserved U0 / Uc (staged with cp.async) -> Uout, and
+//     the FP32 primitives / temperature rewritten in place (W32out, T32out):
+//     the first five cells of a periodic line are re-read by its wrapped end,
+//     so their new primitives are written after the line.
 struct FusedStage {
     int stage;
-    const double *W0[5];    // step-start primitives
-    double *Wout[5];        // new primitives
+    const double *W0[5];
+    double *Wout[5];
     double *Tout;
+    const double *U0[5];
+    const double *Uc[5];
+    double *Uout[5];
+    float *W32out[5];
+    float *T32out;
+    Layout L64;             // layout of the FP64 arrays
     double dt;
     const double *dt_dev;   // non-null: dt from the device time loop
     double gamma, Rgas, dx, vol;
@@ -111,7 +120,8 @@ template <int DIR, typename R, bool CHARW>
 constexpr size_t sweep_smem_bytes() {
     using G = SweepGeom<DIR>;
     return sizeof(R) * ((size_t)G::NLINE * (5 * G::NU + 5 * G::NF + 4 * G::NV + (CHARW ? 5 * G::NU : 0)) +
-                        (size_t)(kRoldSmem ? 14 : 9) * G::CH);
+                        (size_t)(kRoldSmem ? 14 : 9) * G::CH) +
+           ((DIR == 2 && sizeof(R) == 4) ? (size_t)10 * G::CH * sizeof(double) : 0);  // mixed fused stage: U0, Uc
 }
 
 template <typename R>
@@ -174,12 +184,18 @@ sweep_kernel(SweepArgs<R> a) {
     R *const sW = sV + 4 * NL * NV;                  // [5][NL*NU] characteristic bases only
     R *const stg = sW + (USE_W ? 5 * NL * NU : 0);   // [9][CH]
     R *const srold = stg + 9 * CH;                   // [5][CH] (kRoldSmem)
+    // mixed fused stage (float z-sweep only): staged FP64 U0 (rows 0-4), Uc (5-9)
+    double *const sUf = reinterpret_cast<double *>(srold + 5 * CH);
 
     if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
-    // fused stage (FP64 z-sweep): dt, and the thread's CFL minimum / kinetic energy
-    const double fdt = (DIR == 2 && sizeof(R) == 8 && a.fs.stage) ? (a.fs.dt_dev ? *a.fs.dt_dev : a.fs.dt) : 0.0;
+    // fused stage (z-sweep): dt, and the thread's CFL minimum / kinetic energy
+    const double fdt = (DIR == 2 && a.fs.stage) ? (a.fs.dt_dev ? *a.fs.dt_dev : a.fs.dt) : 0.0;
     double cfl_acc = 1e9, ke_acc = 0.0, ke_c = 0.0;  // 1e9: the initial minimum of the CFL reductions
+    // mixed fused stage: the deferred new primitives of one of a periodic line's first five cells
+    bool has_def = false;
+    long def_id = 0;
+    float def_w[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, def_t = 0.f;
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int line = DIR == 0 ? threadIdx.y : threadIdx.x;
     const int ta0 = blockIdx.x * NL + line, tb0 = blockIdx.y;
@@ -274,6 +290,17 @@ sweep_kernel(SweepArgs<R> a) {
             } else {
 #pragma unroll
                 for (int q = 0; q < 5; ++q) rold[q] = a.Rhs[q][cid];
+            }
+        }
+        if constexpr (DIR == 2 && sizeof(R) == 4) {
+            if (a.fs.stage && upd) {  // the FP64 state of the cell this thread updates
+                const long c64 = a.fs.L64.at(ta0 + NG, tb0 + NG, cu);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) cp_async(&sUf[q * CH + ti], a.fs.U0[q] + c64);
+                if (a.fs.stage > 1) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) cp_async(&sUf[(5 + q) * CH + ti], a.fs.Uc[q] + c64);
+                }
             }
         }
         if constexpr (kRoldSmem) cp_async_commit();
@@ -435,6 +462,45 @@ sweep_kernel(SweepArgs<R> a) {
                     fused = true;
                 }
             }
+            if constexpr (DIR == 2 && sizeof(R) == 4) {
+                if (a.fs.stage) {
+                    const FusedStage &f = a.fs;
+                    double U[5];
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) {
+                        const double rr = (double)rq[q];
+                        const double u0 = sUf[q * CH + ti];
+                        const double u = f.stage == 1 ? u0 : sUf[(5 + q) * CH + ti];
+                        U[q] = f.stage == 1 ? u0 + fdt * rr
+                             : f.stage == 2 ? 0.75 * u0 + 0.25 * (u + fdt * rr)
+                                            : (1.0 / 3.0) * u0 + (2.0 / 3.0) * (u + fdt * rr);
+                    }
+                    if (U[0] <= 0.0) U[0] = 1e-12;
+                    double W[5], ir;
+                    c2p_fast(U, f.gamma, W, ir);
+                    const long c64 = f.L64.at(ta0 + NG, tb0 + NG, cu);
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) f.Uout[q][c64] = U[q];
+                    if (per && cu < NG + 5) {  // re-read by the line's wrapped end: write after the line
+                        has_def = true; def_id = cid;
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) def_w[q] = (float)W[q];
+                        def_t = (float)(W[4] * ir / f.Rgas);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) f.W32out[q][cid] = (float)W[q];
+                        f.T32out[cid] = (float)(W[4] * ir / f.Rgas);
+                    }
+                    if (f.stage == 3) {
+                        cfl_acc = fmin(cfl_acc, cfl_bound(U, f.gamma, f.dx));
+                        const double y = 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * f.vol - ke_c;
+                        const double t = __dadd_rn(ke_acc, y);
+                        ke_c = __dsub_rn(__dsub_rn(t, ke_acc), y);
+                        ke_acc = t;
+                    }
+                    fused = true;
+                }
+            }
             if (!fused) {
 #pragma unroll
                 for (int q = 0; q < 5; ++q) a.Rhs[q][cid] = rq[q];
@@ -474,7 +540,14 @@ sweep_kernel(SweepArgs<R> a) {
             }
         }
     }
-    if (DIR == 2 && sizeof(R) == 8 && a.fs.stage == 3)  // uniform: every thread of the block arrives
+    if constexpr (DIR == 2 && sizeof(R) == 4) {
+        if (has_def) {  // the line is done: nothing reads these cells any more
+#pragma unroll
+            for (int q = 0; q < 5; ++q) a.fs.W32out[q][def_id] = def_w[q];
+            a.fs.T32out[def_id] = def_t;
+        }
+    }
+    if (DIR == 2 && a.fs.stage == 3)  // uniform: every thread of the block arrives
         block_min_sum_n<CH>(cfl_acc, ke_acc - ke_c, a.fs.cfl_part + (long)blockIdx.y * gridDim.x + blockIdx.x,
                             a.fs.ke_part + (long)blockIdx.y * gridDim.x + blockIdx.x);
 }
