@@ -1,0 +1,549 @@
+// sweep_pair.cuh -- the mixed path's FP32 sweep with two lines per thread.
+//
+// Same algorithm, chunked shared-memory buffers and boundary handling as
+// sweep_kernel<DIR, float, ...> (sweep.cuh); the difference is the unit of
+// work.  Every thread carries the same face -- and later the same cell -- of
+// two neighbouring lines in the two halves of a float2, so that
+//   * the MDCD detector and linear interpolation, the 6th-order half-node
+//     difference and the viscous derivative run as sm_100's paired FP32
+//     instructions (add / mul / fma on f32x2: one instruction for both lines),
+//   * every shared-memory access moves a 64-bit word (both lines at once), and
+//   * along y and z the two lines are x-neighbours, so the global loads,
+//     stores and cp.async copies are 8 bytes (16 for the FP64 state).
+// The Riemann solvers and the rare WENO branch of the hybrid scheme run per
+// line on the unpacked halves.  The arithmetic of each half is the scalar
+// kernel's; only the placement of fused multiply-adds differs, so results
+// agree with it to FP32 rounding (the mixed path has an accuracy bound, not
+// a bitwise contract).
+//
+// Requires an even number of lines across the block's bundle (ny along x,
+// nx along y and z), so a pair never straddles the end of the domain and the
+// 8-byte accesses stay aligned; sweep_select_f32 falls back to the scalar
+// kernel otherwise and for characteristic reconstruction.
+#pragma once
+
+#include <cstdlib>
+#include <cstring>
+
+#include "sweep.cuh"
+
+namespace ns3d {
+
+__device__ __forceinline__ float2 p2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b, rounded once (b * -1 is exact)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+
+__device__ __forceinline__ void cp_async8(float2 *smem_dst, const float *gsrc) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async16(double2 *smem_dst, const double *gsrc) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+
+// MDCD linear coefficients, each duplicated into both halves
+struct PairConsts {
+    float2 lin[6];
+};
+
+// sum_k c_k f_k (mdcd_linear) for both lines
+__device__ __forceinline__ float2 mdcd_linear2(const float2 *c, float2 f0, float2 f1, float2 f2, float2 f3,
+                                               float2 f4, float2 f5) {
+    float2 s = mul2(c[0], f0);
+    s = fma2(c[1], f1, s);
+    s = fma2(c[2], f2, s);
+    s = fma2(c[3], f3, s);
+    s = fma2(c[4], f4, s);
+    return fma2(c[5], f5, s);
+}
+
+// mdcd_smooth for both lines (the detector of interpolation.cpp:135-209 at
+// one stencil centre): a and b, the sums of two absolute differences, are
+// formed per half (absolute values fold into the scalar adds).
+__device__ __forceinline__ void mdcd_smooth2(float2 fm2, float2 fm1, float2 f0, float2 fp1, float2 fp2, bool &sa,
+                                             bool &sb) {
+    const float eps = float(0.9 * 0.4 / (1.0 - 0.9 * 0.4) * 1e-4);
+    const float2 dm = sub2(f0, fm1), tm = add2(fma2(p2(-2.f), fm1, f0), fm2);
+    const float2 dp = sub2(f0, fp1), tp = add2(fma2(p2(-2.f), fp1, f0), fp2);
+    const float2 A = make_float2(fabsf(dm.x) + fabsf(tm.x), fabsf(dm.y) + fabsf(tm.y));
+    const float2 B = make_float2(fabsf(dp.x) + fabsf(tp.x), fabsf(dp.y) + fabsf(tp.y));
+    const float2 lhs = fma2(mul2(p2(2.f), A), B, p2(eps));
+    const float2 rhs = mul2(p2(0.4f), add2(fma2(A, A, mul2(B, B)), p2(eps)));
+    sa = lhs.x > rhs.x;
+    sb = lhs.y > rhs.y;
+}
+
+// Chunk geometry: C faces of NL = 2 NP lines per chunk, one thread per
+// (line pair, face).  Buffers hold float2 (both lines of a pair):
+//   cells  position p <-> cell fc - 2 + p, p in [0, NU)
+//   faces  position p <-> face fc - 5 + p, p in [0, NF)
+//   visc   position p <-> cell fc - 5 + p, p in [0, NV)
+// Along x a warp owns one pair ([pair][pos]); along y/z the 16 pairs of a
+// bundle span half a warp ([pos][pair]); both give conflict-free 64-bit
+// accesses.
+template <int DIR>
+struct PairGeom {
+    static constexpr int C = DIR == 0 ? 32 : 16;   // faces per chunk
+    static constexpr int NP = DIR == 0 ? 8 : 16;   // line pairs per block
+    static constexpr int NL = 2 * NP;              // lines per block
+    static constexpr int CH = C * NP;              // threads
+    static constexpr int NU = C + 5, NF = C + 7, NV = C + 8;
+    template <int NPOS>
+    __device__ __forceinline__ static int idx(int pair, int pos) {
+        return DIR == 0 ? pair * NPOS + pos : pos * NP + pair;
+    }
+    __device__ __forceinline__ static int tidx(int pair, int slot) {
+        return DIR == 0 ? pair * C + slot : slot * NP + pair;
+    }
+};
+static_assert(PairGeom<2>::NL == SweepGeom<2>::NLINE, "the fused stage's CFL partials assume one z-sweep grid");
+
+// float2 units: U(5) F(5) V(4), staging W(5)+V(4), old RHS(5); z-sweep:
+// FP64 U0, Uc (10 double2) and the deferred primitives of the first five
+// cells of periodic lines (6 x 5 x NP float2)
+template <int DIR>
+constexpr size_t pair_smem_bytes() {
+    using G = PairGeom<DIR>;
+    return 8 * ((size_t)G::NP * (5 * G::NU + 5 * G::NF + 4 * G::NV) + (size_t)14 * G::CH) +
+           (DIR == 2 ? (size_t)10 * G::CH * 16 + (size_t)6 * 5 * G::NP * 8 : 0);
+}
+static_assert((PairGeom<2>::NP * (5 * PairGeom<2>::NU + 5 * PairGeom<2>::NF + 4 * PairGeom<2>::NV) +
+               14 * PairGeom<2>::CH) % 2 == 0, "double2 staging must start 16-byte aligned");
+
+template <int DIR, int INTERP, int RS>
+__global__ void __launch_bounds__(256, 2) sweep_pair_kernel(SweepArgs<float> a, PairConsts pc) {
+    using G = PairGeom<DIR>;
+    constexpr int C = G::C, NP = G::NP, NL = G::NL, CH = G::CH, NU = G::NU, NF = G::NF, NV = G::NV;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2 *const sU = reinterpret_cast<float2 *>(smem_raw);  // [5][NP*NU]
+    float2 *const sF = sU + 5 * NP * NU;                       // [5][NP*NF]
+    float2 *const sV = sF + 5 * NP * NF;                       // [4][NP*NV]
+    float2 *const stg = sV + 4 * NP * NV;                      // [9][CH]
+    float2 *const srold = stg + 9 * CH;                        // [5][CH]
+    double2 *const sUf = reinterpret_cast<double2 *>(srold + 5 * CH);  // [10][CH] z: U0, Uc
+    float2 *const sDef = reinterpret_cast<float2 *>(sUf + 10 * CH);    // [6][5][NP] z: deferred W, T
+
+    if (a.done && *a.done) return;  // uniform over the grid
+    const Layout &L = a.L;
+    const double fdt = (DIR == 2 && a.fs.stage) ? (a.fs.dt_dev ? *a.fs.dt_dev : a.fs.dt) : 0.0;
+    double cfl_acc = 1e9, ke_acc = 0.0, ke_c = 0.0;  // 1e9: the initial minimum of the CFL reductions
+    bool has_def = false;
+    const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
+    const int pr = DIR == 0 ? threadIdx.y : threadIdx.x;
+    const int ta0 = blockIdx.x * NL + 2 * pr, tb0 = blockIdx.y;  // first line of the pair
+    const bool line_ok = ta0 < (DIR == 0 ? L.ny : L.nx);          // both lines (even count)
+    const int n = DIR == 0 ? L.nx : (DIR == 1 ? L.ny : L.nz);
+    // padded-layout address of cell c of the first line; the second line is
+    // lpair (vpair for the node fluxes) further on
+    long lbase, lstride, lpair, vbase, vstride, vpair;
+    if (DIR == 0) {
+        lbase = L.at(0, ta0 + NG, tb0 + NG); lstride = 1; lpair = L.px;
+        vbase = ((long)tb0 * L.ny + ta0) * L.nx; vstride = 1; vpair = L.nx;
+    } else if (DIR == 1) {
+        lbase = L.at(ta0 + NG, 0, tb0 + NG); lstride = L.px; lpair = 1;
+        vbase = (long)tb0 * L.ny * L.nx + ta0; vstride = L.nx; vpair = 1;
+    } else {
+        lbase = L.at(ta0 + NG, tb0 + NG, 0); lstride = (long)L.px * L.sy; lpair = 1;
+        vbase = (long)tb0 * L.nx + ta0; vstride = (long)L.nx * L.ny; vpair = 1;
+    }
+    const bool per = a.periodic != 0;
+    const bool visc = a.visc != 0;
+    const bool rmw = a.first == 0;
+    const int fb = per ? 0 : NG - 1;
+    const int fe = per ? n + 5 : n + NG;
+    const int cell_end = per ? n + 8 : n + 6;
+    const int chunk_end = n + NG + 2;
+    const int ti = G::tidx(pr, slot);
+    const float gm1 = a.sp.gamma - 1.f;
+
+    auto wrap = [&](int c) { return per ? (c < NG ? c + n : (c >= n + NG ? c - n : c)) : c; };
+    auto vis_pos = [&](int c) -> int {
+        if (c < 0) return -1;
+        int ci = c - NG;
+        if (per) { if (ci < 0) ci += n; else if (ci >= n) ci -= n; return ci; }
+        return (ci >= 0 && ci < n) ? ci : -1;
+    };
+    auto ld2 = [&](const float *p, long off) -> float2 {
+        if (DIR == 0) return make_float2(p[0], p[off]);
+        return *reinterpret_cast<const float2 *>(p);
+    };
+    auto cp2 = [&](float2 *dst, const float *src, long off) {
+        if (DIR == 0) { cp_async(&dst->x, src); cp_async(&dst->y, src + off); }
+        else cp_async8(dst, src);
+    };
+    auto st2 = [&](float *p, long off, float2 v) {
+        if (DIR == 0) { p[0] = v.x; p[off] = v.y; }
+        else *reinterpret_cast<float2 *>(p) = v;
+    };
+    auto put_cell = [&](int pu, int pv, const float2 *w5, const float2 *vf) {
+        float Ua[5], Ub[5];
+        p2c_f(w5[0].x, w5[1].x, w5[2].x, w5[3].x, w5[4].x, gm1, Ua);
+        p2c_f(w5[0].y, w5[1].y, w5[2].y, w5[3].y, w5[4].y, gm1, Ub);
+        const int s = G::template idx<NU>(pr, pu);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) sU[q * NP * NU + s] = make_float2(Ua[q], Ub[q]);
+        if (visc && pv >= 0) {
+            const int sv = G::template idx<NV>(pr, pv);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sV[q * NP * NV + sv] = vf[q];
+        }
+    };
+
+    // ---- first chunk: visc positions [0, NV) = cells fb-5 .., cell
+    //      positions [0, NU) = cells fb-2 .. (position p-3 of the same cell)
+    if (line_ok) {
+        for (int p = slot; p < NV; p += C) {
+            const int c = fb - 5 + p;
+            float2 vf[4] = {p2(0.f), p2(0.f), p2(0.f), p2(0.f)};
+            if (visc) {
+                const int ci = vis_pos(c);
+                if (ci >= 0) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) vf[q] = ld2(a.V[q] + vbase + ci * vstride, vpair);
+                }
+            }
+            if (p >= 3 && c < cell_end) {
+                const long id = lbase + wrap(c) * lstride;
+                float2 w5[5];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) w5[q] = ld2(a.W[q] + id, lpair);
+                put_cell(p - 3, p, w5, vf);
+            } else if (visc) {
+                const int sv = G::template idx<NV>(pr, p);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) sV[q * NP * NV + sv] = vf[q];
+            }
+        }
+    }
+
+    for (int fc = fb; fc < chunk_end; fc += C) {
+        // cell updated by this thread (both lines) in this chunk
+        const int cu = fc - 2 + slot;
+        const bool upd = line_ok && cu >= NG && cu < n + NG;
+        const long cid = lbase + cu * lstride;
+        if (rmw && upd) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) cp2(&srold[q * CH + ti], a.Rhs[q] + cid, lpair);
+        }
+        if constexpr (DIR == 2) {
+            if (a.fs.stage && upd) {  // the FP64 state of the two cells this thread updates
+                const long c64 = a.fs.L64.at(ta0 + NG, tb0 + NG, cu);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) cp_async16(&sUf[q * CH + ti], a.fs.U0[q] + c64);
+                if (a.fs.stage > 1) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) cp_async16(&sUf[(5 + q) * CH + ti], a.fs.Uc[q] + c64);
+                }
+            }
+        }
+        cp_async_commit();
+        // stage the next chunk's new cell (cell and visc positions 5+slot, 8+slot)
+        const int cn = fc + C + 3 + slot;
+        const bool stage = fc + C < chunk_end && line_ok && cn < cell_end;
+        if (stage) {
+            const long id = lbase + wrap(cn) * lstride;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) cp2(&stg[q * CH + ti], a.W[q] + id, lpair);
+            if (visc) {
+                const int ci = vis_pos(cn);
+                if (ci >= 0) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) cp2(&stg[(5 + q) * CH + ti], a.V[q] + vbase + ci * vstride, vpair);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) stg[(5 + q) * CH + ti] = p2(0.f);
+                }
+            }
+        }
+        cp_async_commit();
+        __syncthreads();  // buffers of this chunk complete
+
+        // ---- face f = fc + slot of both lines: cell positions slot .. slot+5
+        const int f = fc + slot;
+        if (line_ok && f < fe) {
+            float2 st[5][6];
+#pragma unroll
+            for (int q = 0; q < 5; ++q)
+#pragma unroll
+                for (int m = 0; m < 6; ++m) st[q][m] = sU[q * NP * NU + G::template idx<NU>(pr, slot + m)];
+            float2 UL[5], UR[5];
+            if constexpr (INTERP == I_MDCD_HYBRID || INTERP == I_MDCD_LINEAR) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    UL[q] = mdcd_linear2(pc.lin, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]);
+                    UR[q] = mdcd_linear2(pc.lin, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1], st[q][0]);
+                }
+            }
+            if constexpr (INTERP == I_MDCD_HYBRID) {
+                // detectors of both lines; the WENO branch per line where one rejected
+                unsigned wa = 0, wb = 0;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    bool a2, b2, a3, b3;
+                    mdcd_smooth2(st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], a2, b2);
+                    mdcd_smooth2(st[q][1], st[q][2], st[q][3], st[q][4], st[q][5], a3, b3);
+                    wa |= ((a2 && a3) ? 0u : 1u) << q;
+                    wb |= ((b2 && b3) ? 0u : 1u) << q;
+                }
+                if (wa | wb) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) {
+                        if (wa & (1u << q)) {
+                            UL[q].x = mdcd_weno_branch(a.sp.hd, st[q][0].x, st[q][1].x, st[q][2].x, st[q][3].x,
+                                                       st[q][4].x, st[q][5].x);
+                            UR[q].x = mdcd_weno_branch(a.sp.hd, st[q][5].x, st[q][4].x, st[q][3].x, st[q][2].x,
+                                                       st[q][1].x, st[q][0].x);
+                        }
+                        if (wb & (1u << q)) {
+                            UL[q].y = mdcd_weno_branch(a.sp.hd, st[q][0].y, st[q][1].y, st[q][2].y, st[q][3].y,
+                                                       st[q][4].y, st[q][5].y);
+                            UR[q].y = mdcd_weno_branch(a.sp.hd, st[q][5].y, st[q][4].y, st[q][3].y, st[q][2].y,
+                                                       st[q][1].y, st[q][0].y);
+                        }
+                    }
+                }
+            } else if constexpr (INTERP != I_MDCD_LINEAR) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    float sa[6], sb[6];
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) { sa[m] = st[q][m].x; sb[m] = st[q][m].y; }
+                    face_pair<float, INTERP>(a.sp, sa, UL[q].x, UR[q].x);
+                    face_pair<float, INTERP>(a.sp, sb, UL[q].y, UR[q].y);
+                }
+            }
+            float ULa[5], URa[5], ULb[5], URb[5], Fa[5], Fb[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { ULa[q] = UL[q].x; URa[q] = UR[q].x; ULb[q] = UL[q].y; URb[q] = UR[q].y; }
+            riemann<DIR, float, RS>(a.sp, ULa, URa, Fa);
+            riemann<DIR, float, RS>(a.sp, ULb, URb, Fb);
+            const int s = G::template idx<NF>(pr, slot + 5);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) sF[q * NP * NF + s] = make_float2(Fa[q], Fb[q]);
+        }
+        cp_async_wait<1>();  // this thread's old-RHS / FP64-state copies landed
+        __syncthreads();     // faces of this chunk complete
+        float2 rold[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) rold[q] = (rmw && upd) ? srold[q * CH + ti] : p2(0.f);
+
+        // ---- cell cu of both lines: faces cu-3 .. cu+2 at positions slot ..
+        //      slot+5, node fluxes cu-3 .. cu+3 at visc positions slot .. slot+6
+        if (upd) {
+            const bool edge = !per && (cu - NG < 3 || cu - NG >= n - 3);
+            float2 d[5], vd[4] = {p2(0.f), p2(0.f), p2(0.f), p2(0.f)};
+            if (!edge) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    const float2 *fq = sF + q * NP * NF;
+                    auto F_ = [&](int m) { return fq[G::template idx<NF>(pr, slot + m)]; };
+                    // diff_6th_central_half, InviscousFlux.cpp:990-992
+                    float2 t = mul2(sub2(F_(3), F_(2)), p2(float(75.0 / 64.0)));
+                    t = fma2(sub2(F_(4), F_(1)), p2(float(-25.0 / 384.0)), t);
+                    t = fma2(sub2(F_(5), F_(0)), p2(float(3.0 / 640.0)), t);
+                    d[q] = mul2(t, p2(a.inv_h));
+                }
+                if (visc) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 *vq = sV + q * NP * NV;
+                        auto V_ = [&](int off) { return vq[G::template idx<NV>(pr, slot + 3 + off)]; };
+                        float2 t = fma2(p2(-9.f), V_(2), V_(3));
+                        t = fma2(p2(45.f), V_(1), t);
+                        t = fma2(p2(-45.f), V_(-1), t);
+                        t = fma2(p2(9.f), V_(-2), t);
+                        vd[q] = mul2(sub2(t, V_(-3)), p2(a.dinv[2]));
+                    }
+                }
+            } else {
+                // within 3 cells of a non-periodic boundary: ghost faces and
+                // reduced viscous orders as the scalar kernel, per line
+                const int pf_lo = (NG - 1) - (fc - 5), pf_hi = (n + NG - 1) - (fc - 5);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    float2 fv[6];
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) {
+                        int pm = slot + m;
+                        bool zero = false;
+                        const int ff = cu - 3 + m;
+                        if (ff < NG - 1) { if (a.outflow_lo) pm = pf_lo; else zero = true; }
+                        else if (ff > n + NG - 1) { if (a.outflow_hi) pm = pf_hi; else zero = true; }
+                        fv[m] = zero ? p2(0.f) : sF[q * NP * NF + G::template idx<NF>(pr, pm)];
+                    }
+                    float2 t = mul2(sub2(fv[3], fv[2]), p2(float(75.0 / 64.0)));
+                    t = fma2(sub2(fv[4], fv[1]), p2(float(-25.0 / 384.0)), t);
+                    t = fma2(sub2(fv[5], fv[0]), p2(float(3.0 / 640.0)), t);
+                    d[q] = mul2(t, p2(a.inv_h));
+                }
+                if (visc) {
+                    const int o = visc_order(cu - NG, n, false);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 *vq = sV + q * NP * NV;
+                        vd[q].x = dstencil_inv<float>(
+                            [&](int off) { return vq[G::template idx<NV>(pr, slot + 3 + off)].x; }, o, a.dinv);
+                        vd[q].y = dstencil_inv<float>(
+                            [&](int off) { return vq[G::template idx<NV>(pr, slot + 3 + off)].y; }, o, a.dinv);
+                    }
+                }
+            }
+            float2 rq[5];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                rq[q] = sub2(rold[q], d[q]);
+                if (q > 0) rq[q] = add2(rq[q], vd[q - 1]);
+            }
+            bool fused = false;
+            if constexpr (DIR == 2) {
+                if (a.fs.stage) {
+                    // runge_kutta_3's update of both cells in FP64 (range_kutta.cpp:53-91)
+                    const FusedStage &fs = a.fs;
+                    const long c64 = fs.L64.at(ta0 + NG, tb0 + NG, cu);
+                    double2 Uo[5];
+                    float2 Wn[5], Tn;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        double U[5];
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) {
+                            const double rr = (double)(h ? rq[q].y : rq[q].x);
+                            const double2 s0 = sUf[q * CH + ti];
+                            const double u0 = h ? s0.y : s0.x;
+                            double u = u0;
+                            if (fs.stage > 1) { const double2 s1 = sUf[(5 + q) * CH + ti]; u = h ? s1.y : s1.x; }
+                            U[q] = fs.stage == 1 ? u0 + fdt * rr
+                                 : fs.stage == 2 ? 0.75 * u0 + 0.25 * (u + fdt * rr)
+                                                 : (1.0 / 3.0) * u0 + (2.0 / 3.0) * (u + fdt * rr);
+                        }
+                        if (U[0] <= 0.0) U[0] = 1e-12;
+                        double W[5], ir;
+                        c2p_fast(U, fs.gamma, W, ir);
+                        const float t = (float)(W[4] * ir / fs.Rgas);
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) {
+                            if (h) { Uo[q].y = U[q]; Wn[q].y = (float)W[q]; }
+                            else { Uo[q].x = U[q]; Wn[q].x = (float)W[q]; }
+                        }
+                        if (h) Tn.y = t; else Tn.x = t;
+                        if (fs.stage == 3) {
+                            cfl_acc = fmin(cfl_acc, cfl_bound(U, fs.gamma, fs.dx));
+                            const double y = 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * fs.vol - ke_c;
+                            const double tk = __dadd_rn(ke_acc, y);
+                            ke_c = __dsub_rn(__dsub_rn(tk, ke_acc), y);
+                            ke_acc = tk;
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) *reinterpret_cast<double2 *>(fs.Uout[q] + c64) = Uo[q];
+                    if (per && cu < NG + 5) {  // re-read by the line's wrapped end: write after the line
+                        has_def = true;
+                        const int dp = (cu - NG) * NP + pr;
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) sDef[q * 5 * NP + dp] = Wn[q];
+                        sDef[5 * 5 * NP + dp] = Tn;
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) *reinterpret_cast<float2 *>(fs.W32out[q] + cid) = Wn[q];
+                        *reinterpret_cast<float2 *>(fs.T32out + cid) = Tn;
+                    }
+                    fused = true;
+                }
+            }
+            if (!fused) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) st2(a.Rhs[q] + cid, lpair, rq[q]);
+            }
+        }
+        cp_async_wait<0>();
+        __syncthreads();  // buffer reads of this chunk done; staged cells landed
+
+        // ---- move the tails to the front, append the staged cell
+        if (line_ok && fc + C < chunk_end) {
+            if (visc && slot >= C - 8) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    sV[q * NP * NV + G::template idx<NV>(pr, slot - C + 8)] =
+                        sV[q * NP * NV + G::template idx<NV>(pr, slot + 8)];
+            }
+            if (slot >= C - 5) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    sU[q * NP * NU + G::template idx<NU>(pr, slot - C + 5)] =
+                        sU[q * NP * NU + G::template idx<NU>(pr, slot + 5)];
+                    sF[q * NP * NF + G::template idx<NF>(pr, slot - C + 5)] =
+                        sF[q * NP * NF + G::template idx<NF>(pr, slot + 5)];
+                }
+            }
+            if (stage) {
+                float2 w5[5], v4[4] = {p2(0.f), p2(0.f), p2(0.f), p2(0.f)};
+#pragma unroll
+                for (int q = 0; q < 5; ++q) w5[q] = stg[q * CH + ti];
+                if (visc) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) v4[q] = stg[(5 + q) * CH + ti];
+                }
+                put_cell(5 + slot, 8 + slot, w5, v4);
+            }
+        }
+    }
+    if constexpr (DIR == 2) {
+        if (has_def) {  // the line is done: nothing reads these cells any more
+            // the thread deferred its cells of the first chunk: cu = fb - 2 + slot
+            const int cu = fb - 2 + slot;
+            const long cid = lbase + cu * lstride;
+            const int dp = (cu - NG) * NP + pr;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) *reinterpret_cast<float2 *>(a.fs.W32out[q] + cid) = sDef[q * 5 * NP + dp];
+            *reinterpret_cast<float2 *>(a.fs.T32out + cid) = sDef[5 * 5 * NP + dp];
+        }
+        if (a.fs.stage == 3)  // uniform: every thread of the block arrives
+            block_min_sum_n<CH>(cfl_acc, ke_acc - ke_c, a.fs.cfl_part + (long)blockIdx.y * gridDim.x + blockIdx.x,
+                                a.fs.ke_part + (long)blockIdx.y * gridDim.x + blockIdx.x);
+    }
+}
+
+template <int DIR, int INTERP, int RS>
+inline cudaError_t launch_pair(const SweepArgs<float> &a, cudaStream_t st) {
+    using G = PairGeom<DIR>;
+    dim3 block(DIR == 0 ? G::C : G::NP, DIR == 0 ? G::NP : G::C);
+    dim3 grid(((DIR == 0 ? a.L.ny : a.L.nx) + G::NL - 1) / G::NL, DIR == 2 ? a.L.ny : a.L.nz);
+    const size_t smem = pair_smem_bytes<DIR>();
+    static unsigned configured = 0;  // one bit per device ordinal
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured & (1u << (dev & 31)))) {
+        cudaError_t e = cudaFuncSetAttribute(sweep_pair_kernel<DIR, INTERP, RS>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured |= 1u << (dev & 31);
+    }
+    PairConsts pc;
+    for (int k = 0; k < 6; ++k) pc.lin[k] = make_float2(a.sp.lin[k], a.sp.lin[k]);
+    sweep_pair_kernel<DIR, INTERP, RS><<<grid, block, smem, st>>>(a, pc);
+    return cudaGetLastError();
+}
+
+// NS3D_SWEEP32=scalar selects the one-line-per-thread FP32 kernel (kept for
+// characteristic reconstruction and odd line counts, and for comparison).
+inline bool sweep32_scalar_forced() {
+    const char *v = std::getenv("NS3D_SWEEP32");
+    return v && std::strcmp(v, "scalar") == 0;
+}
+
+template <int DIR>
+inline cudaError_t sweep_select_f32(const SweepArgs<float> &a, cudaStream_t st) {
+    const auto &sp = a.sp;
+    const int across = DIR == 0 ? a.L.ny : a.L.nx;
+    if (sp.char_recon || (across & 1) || sweep32_scalar_forced()) return sweep_select<DIR, float>(a, st);
+    if (sp.interp == I_WENO5 && sp.riemann == R_ROE) return launch_pair<DIR, I_WENO5, R_ROE>(a, st);
+    if (sp.interp == I_MDCD_HYBRID && sp.riemann == R_HLLC) return launch_pair<DIR, I_MDCD_HYBRID, R_HLLC>(a, st);
+    if (sp.interp == I_MDCD_LINEAR && sp.riemann == R_HLLC) return launch_pair<DIR, I_MDCD_LINEAR, R_HLLC>(a, st);
+    return launch_pair<DIR, RUNTIME, RUNTIME>(a, st);
+}
+
+}  // namespace ns3d
