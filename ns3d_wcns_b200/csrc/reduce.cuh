@@ -89,6 +89,33 @@ __device__ __forceinline__ void block_min_sum_n(double m, double v, double *out_
     }
 }
 
+// The CFL bound of a block from its largest wave speed: min_i fl(dx / s_i)
+// equals fl(dx / max_i s_i) bit for bit (correctly rounded division by a
+// positive speed is monotone; fmin and fmax both skip NaN), so the fused
+// stage keeps max s per thread and divides once per block.  Capped at 1e9,
+// the initial value of the per-cell minimum.  Thread 0 writes both results.
+template <int NT>
+__device__ __forceinline__ void block_speed_sum_n(double s, double v, double dx, double *out_min,
+                                                  double *out_sum) {
+    __shared__ double shm[NT / 32], shs[NT / 32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s = fmax(s, __shfl_down_sync(0xffffffffu, s, o));
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    if (lane == 0) { shm[wid] = s; shs[wid] = v; }
+    __syncthreads();
+    if (tid == 0) {
+        double a = shm[0], b = shs[0];
+#pragma unroll
+        for (int w = 1; w < NT / 32; ++w) { a = fmax(a, shm[w]); b += shs[w]; }
+        *out_min = fmin(1e9, dx / a);
+        *out_sum = b;
+    }
+}
+
 // Per-cell CFL bound of compute_timestep (timestep.cpp:12-20) from the FP64
 // conserved state: u = rhou/rho, p = (gamma-1)(E - 0.5 rho u^2) (v, w are not
 // used), a = sqrt(gamma p / rho), bound = dx / (|u| + a).
@@ -98,6 +125,15 @@ __device__ __forceinline__ double cfl_bound(const double U[5], double gamma, dou
     double p = __dmul_rn(gamma - 1., __dsub_rn(U[4], __dmul_rn(__dmul_rn(__dmul_rn(0.5, rho), u), u)));
     double a = sqrt(__dmul_rn(gamma, p) / rho);
     return dx / __dadd_rn(fabs(u), a);
+}
+
+// The wave speed |u| + a of cfl_bound (cfl_bound = dx / cfl_speed, same bits).
+__device__ __forceinline__ double cfl_speed(const double U[5], double gamma) {
+    double rho = U[0];
+    double u = U[1] / rho;
+    double p = __dmul_rn(gamma - 1., __dsub_rn(U[4], __dmul_rn(__dmul_rn(__dmul_rn(0.5, rho), u), u)));
+    double a = sqrt(__dmul_rn(gamma, p) / rho);
+    return __dadd_rn(fabs(u), a);
 }
 
 }  // namespace ns3d

@@ -149,7 +149,7 @@ __device__ __forceinline__ R dstencil_inv(F f, int order, const R *dinv) {
 // right-hand side r and current conserved state Uc (the sweep's exact p2c of
 // W): the operations of stage_kernel64 for an interior cell, so the same bits.
 __device__ __forceinline__ void fused_stage_cell(const FusedStage &f, double dt, long c, const double *r,
-                                                 const double *Ucur, double &cfl, double &ke, double &kc) {
+                                                 const double *Ucur, double &smax, double &ke, double &kc) {
     double U0[5], U[5], W[5];
     p2c_exact(f.W0[0][c], f.W0[1][c], f.W0[2][c], f.W0[3][c], f.W0[4][c], f.gamma, U0);
 #pragma unroll
@@ -161,7 +161,7 @@ __device__ __forceinline__ void fused_stage_cell(const FusedStage &f, double dt,
     if (f.stage == 3) {
         double Un[5];
         p2c_exact(W[0], W[1], W[2], W[3], W[4], f.gamma, Un);
-        cfl = fmin(cfl, cfl_bound(Un, f.gamma, f.dx));
+        smax = fmax(smax, cfl_speed(Un, f.gamma));  // largest wave speed: one division per block
         // a thread adds one cell per chunk along its line: compensated
         // (Kahan) summation keeps its partial exact to rounding
         const double y = 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * f.vol - kc;
@@ -189,9 +189,10 @@ sweep_kernel(SweepArgs<R> a) {
 
     if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
-    // fused stage (z-sweep): dt, and the thread's CFL minimum / kinetic energy
+    // fused stage (z-sweep): dt, and the thread's largest wave speed / kinetic energy
     const double fdt = (DIR == 2 && a.fs.stage) ? (a.fs.dt_dev ? *a.fs.dt_dev : a.fs.dt) : 0.0;
-    double cfl_acc = 1e9, ke_acc = 0.0, ke_c = 0.0;  // 1e9: the initial minimum of the CFL reductions
+    double cfl_acc = 0.0, ke_acc = 0.0, ke_c = 0.0;  // largest wave speed, kinetic energy
+    const double irg = (DIR == 2 && sizeof(R) == 4 && a.fs.stage) ? 1.0 / a.fs.Rgas : 0.0;  // mixed: T = p / (rho Rgas)
     // mixed fused stage: the deferred new primitives of one of a periodic line's first five cells
     bool has_def = false;
     long def_id = 0;
@@ -485,14 +486,14 @@ sweep_kernel(SweepArgs<R> a) {
                         has_def = true; def_id = cid;
 #pragma unroll
                         for (int q = 0; q < 5; ++q) def_w[q] = (float)W[q];
-                        def_t = (float)(W[4] * ir / f.Rgas);
+                        def_t = (float)(W[4] * ir * irg);
                     } else {
 #pragma unroll
                         for (int q = 0; q < 5; ++q) f.W32out[q][cid] = (float)W[q];
-                        f.T32out[cid] = (float)(W[4] * ir / f.Rgas);
+                        f.T32out[cid] = (float)(W[4] * ir * irg);
                     }
                     if (f.stage == 3) {
-                        cfl_acc = fmin(cfl_acc, cfl_bound(U, f.gamma, f.dx));
+                        cfl_acc = fmax(cfl_acc, cfl_speed(U, f.gamma));
                         const double y = 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * f.vol - ke_c;
                         const double t = __dadd_rn(ke_acc, y);
                         ke_c = __dsub_rn(__dsub_rn(t, ke_acc), y);
@@ -548,8 +549,9 @@ sweep_kernel(SweepArgs<R> a) {
         }
     }
     if (DIR == 2 && a.fs.stage == 3)  // uniform: every thread of the block arrives
-        block_min_sum_n<CH>(cfl_acc, ke_acc - ke_c, a.fs.cfl_part + (long)blockIdx.y * gridDim.x + blockIdx.x,
-                            a.fs.ke_part + (long)blockIdx.y * gridDim.x + blockIdx.x);
+        block_speed_sum_n<CH>(cfl_acc, ke_acc - ke_c, a.fs.dx,
+                              a.fs.cfl_part + (long)blockIdx.y * gridDim.x + blockIdx.x,
+                              a.fs.ke_part + (long)blockIdx.y * gridDim.x + blockIdx.x);
 }
 
 template <int DIR, typename R, int INTERP, int RS, int CHAR>

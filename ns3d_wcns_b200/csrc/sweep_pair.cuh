@@ -114,8 +114,17 @@ constexpr size_t pair_smem_bytes() {
 static_assert((PairGeom<2>::NP * (5 * PairGeom<2>::NU + 5 * PairGeom<2>::NF + 4 * PairGeom<2>::NV) +
                14 * PairGeom<2>::CH) % 2 == 0, "double2 staging must start 16-byte aligned");
 
+// resident blocks per SM requested from the register allocator: three along
+// x (80 registers, 63 KB of shared memory; 0.50 -> 0.46 ms at 256^3), two
+// along y and z (the z-sweep's fused stage needs its registers, and 111 KB of
+// shared memory per block allow two).  The shared-memory carveout is left to
+// the driver: forcing the largest one (smallest L1) slowed the x and y
+// sweeps by 10-25 %.
+template <int DIR>
+constexpr int pair_min_blocks() { return DIR == 0 ? 3 : 2; }
+
 template <int DIR, int INTERP, int RS>
-__global__ void __launch_bounds__(256, 2) sweep_pair_kernel(SweepArgs<float> a, PairConsts pc) {
+__global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel(SweepArgs<float> a, PairConsts pc) {
     using G = PairGeom<DIR>;
     constexpr int C = G::C, NP = G::NP, NL = G::NL, CH = G::CH, NU = G::NU, NF = G::NF, NV = G::NV;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -130,7 +139,8 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(SweepArgs<float> a, 
     if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
     const double fdt = (DIR == 2 && a.fs.stage) ? (a.fs.dt_dev ? *a.fs.dt_dev : a.fs.dt) : 0.0;
-    double cfl_acc = 1e9, ke_acc = 0.0, ke_c = 0.0;  // 1e9: the initial minimum of the CFL reductions
+    double cfl_acc = 0.0, ke_acc = 0.0, ke_c = 0.0;  // largest wave speed, kinetic energy
+    const double irg = (DIR == 2 && a.fs.stage) ? 1.0 / a.fs.Rgas : 0.0;  // T = p / (rho Rgas)
     bool has_def = false;
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int pr = DIR == 0 ? threadIdx.y : threadIdx.x;
@@ -265,55 +275,51 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(SweepArgs<float> a, 
         // ---- face f = fc + slot of both lines: cell positions slot .. slot+5
         const int f = fc + slot;
         if (line_ok && f < fe) {
-            float2 st[5][6];
-#pragma unroll
-            for (int q = 0; q < 5; ++q)
-#pragma unroll
-                for (int m = 0; m < 6; ++m) st[q][m] = sU[q * NP * NU + G::template idx<NU>(pr, slot + m)];
+            // one variable's stencil at a time (its registers die with it);
+            // the rare WENO branch re-reads its stencil from shared memory
             float2 UL[5], UR[5];
-            if constexpr (INTERP == I_MDCD_HYBRID || INTERP == I_MDCD_LINEAR) {
+            unsigned wa = 0, wb = 0;
 #pragma unroll
-                for (int q = 0; q < 5; ++q) {
-                    UL[q] = mdcd_linear2(pc.lin, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]);
-                    UR[q] = mdcd_linear2(pc.lin, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1], st[q][0]);
+            for (int q = 0; q < 5; ++q) {
+                float2 sq[6];
+#pragma unroll
+                for (int m = 0; m < 6; ++m) sq[m] = sU[q * NP * NU + G::template idx<NU>(pr, slot + m)];
+                if constexpr (INTERP == I_MDCD_HYBRID || INTERP == I_MDCD_LINEAR) {
+                    UL[q] = mdcd_linear2(pc.lin, sq[0], sq[1], sq[2], sq[3], sq[4], sq[5]);
+                    UR[q] = mdcd_linear2(pc.lin, sq[5], sq[4], sq[3], sq[2], sq[1], sq[0]);
+                }
+                if constexpr (INTERP == I_MDCD_HYBRID) {
+                    // detectors of both lines at the face's two central cells
+                    bool a2, b2, a3, b3;
+                    mdcd_smooth2(sq[0], sq[1], sq[2], sq[3], sq[4], a2, b2);
+                    mdcd_smooth2(sq[1], sq[2], sq[3], sq[4], sq[5], a3, b3);
+                    wa |= ((a2 && a3) ? 0u : 1u) << q;
+                    wb |= ((b2 && b3) ? 0u : 1u) << q;
+                } else if constexpr (INTERP != I_MDCD_LINEAR) {
+                    float sa[6], sb[6];
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) { sa[m] = sq[m].x; sb[m] = sq[m].y; }
+                    face_pair<float, INTERP>(a.sp, sa, UL[q].x, UR[q].x);
+                    face_pair<float, INTERP>(a.sp, sb, UL[q].y, UR[q].y);
                 }
             }
             if constexpr (INTERP == I_MDCD_HYBRID) {
-                // detectors of both lines; the WENO branch per line where one rejected
-                unsigned wa = 0, wb = 0;
-#pragma unroll
-                for (int q = 0; q < 5; ++q) {
-                    bool a2, b2, a3, b3;
-                    mdcd_smooth2(st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], a2, b2);
-                    mdcd_smooth2(st[q][1], st[q][2], st[q][3], st[q][4], st[q][5], a3, b3);
-                    wa |= ((a2 && a3) ? 0u : 1u) << q;
-                    wb |= ((b2 && b3) ? 0u : 1u) << q;
-                }
-                if (wa | wb) {
+                if (wa | wb) {  // the WENO branch of the lines whose detector rejected the linear scheme
 #pragma unroll
                     for (int q = 0; q < 5; ++q) {
-                        if (wa & (1u << q)) {
-                            UL[q].x = mdcd_weno_branch(a.sp.hd, st[q][0].x, st[q][1].x, st[q][2].x, st[q][3].x,
-                                                       st[q][4].x, st[q][5].x);
-                            UR[q].x = mdcd_weno_branch(a.sp.hd, st[q][5].x, st[q][4].x, st[q][3].x, st[q][2].x,
-                                                       st[q][1].x, st[q][0].x);
-                        }
-                        if (wb & (1u << q)) {
-                            UL[q].y = mdcd_weno_branch(a.sp.hd, st[q][0].y, st[q][1].y, st[q][2].y, st[q][3].y,
-                                                       st[q][4].y, st[q][5].y);
-                            UR[q].y = mdcd_weno_branch(a.sp.hd, st[q][5].y, st[q][4].y, st[q][3].y, st[q][2].y,
-                                                       st[q][1].y, st[q][0].y);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            if ((h ? wb : wa) & (1u << q)) {
+                                const volatile float *vq = reinterpret_cast<const volatile float *>(sU + q * NP * NU);
+                                float f[6];
+#pragma unroll
+                                for (int m = 0; m < 6; ++m) f[m] = vq[2 * G::template idx<NU>(pr, slot + m) + h];
+                                const float l = mdcd_weno_branch(a.sp.hd, f[0], f[1], f[2], f[3], f[4], f[5]);
+                                const float r = mdcd_weno_branch(a.sp.hd, f[5], f[4], f[3], f[2], f[1], f[0]);
+                                if (h) { UL[q].y = l; UR[q].y = r; } else { UL[q].x = l; UR[q].x = r; }
+                            }
                         }
                     }
-                }
-            } else if constexpr (INTERP != I_MDCD_LINEAR) {
-#pragma unroll
-                for (int q = 0; q < 5; ++q) {
-                    float sa[6], sb[6];
-#pragma unroll
-                    for (int m = 0; m < 6; ++m) { sa[m] = st[q][m].x; sb[m] = st[q][m].y; }
-                    face_pair<float, INTERP>(a.sp, sa, UL[q].x, UR[q].x);
-                    face_pair<float, INTERP>(a.sp, sb, UL[q].y, UR[q].y);
                 }
             }
             float ULa[5], URa[5], ULb[5], URb[5], Fa[5], Fb[5];
@@ -423,7 +429,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(SweepArgs<float> a, 
                         if (U[0] <= 0.0) U[0] = 1e-12;
                         double W[5], ir;
                         c2p_fast(U, fs.gamma, W, ir);
-                        const float t = (float)(W[4] * ir / fs.Rgas);
+                        const float t = (float)(W[4] * ir * irg);
 #pragma unroll
                         for (int q = 0; q < 5; ++q) {
                             if (h) { Uo[q].y = U[q]; Wn[q].y = (float)W[q]; }
@@ -431,7 +437,7 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(SweepArgs<float> a, 
                         }
                         if (h) Tn.y = t; else Tn.x = t;
                         if (fs.stage == 3) {
-                            cfl_acc = fmin(cfl_acc, cfl_bound(U, fs.gamma, fs.dx));
+                            cfl_acc = fmax(cfl_acc, cfl_speed(U, fs.gamma));
                             const double y = 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * fs.vol - ke_c;
                             const double tk = __dadd_rn(ke_acc, y);
                             ke_c = __dsub_rn(__dsub_rn(tk, ke_acc), y);
@@ -502,8 +508,9 @@ __global__ void __launch_bounds__(256, 2) sweep_pair_kernel(SweepArgs<float> a, 
             *reinterpret_cast<float2 *>(a.fs.T32out + cid) = sDef[5 * 5 * NP + dp];
         }
         if (a.fs.stage == 3)  // uniform: every thread of the block arrives
-            block_min_sum_n<CH>(cfl_acc, ke_acc - ke_c, a.fs.cfl_part + (long)blockIdx.y * gridDim.x + blockIdx.x,
-                                a.fs.ke_part + (long)blockIdx.y * gridDim.x + blockIdx.x);
+            block_speed_sum_n<CH>(cfl_acc, ke_acc - ke_c, a.fs.dx,
+                                  a.fs.cfl_part + (long)blockIdx.y * gridDim.x + blockIdx.x,
+                                  a.fs.ke_part + (long)blockIdx.y * gridDim.x + blockIdx.x);
     }
 }
 
