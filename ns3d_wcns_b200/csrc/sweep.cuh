@@ -196,6 +196,9 @@ sweep_kernel(SweepArgs<R> a) {
     // mixed fused stage: the deferred new primitives of one of a periodic line's first five cells
     bool has_def = false;
     long def_id = 0;
+    unsigned det_carry = 0;  // x-sweep detector bits of the previous chunk's last face (cell fc)
+    // y/z-sweep detector bits, position p <-> cell fc + p (MDCD_HYBRID)
+    __shared__ unsigned char sDet[(DIR != 0 && CHAR == 0 && INTERP == I_MDCD_HYBRID) ? (C + 1) * NL : 1];
     float def_w[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, def_t = 0.f;
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int line = DIR == 0 ? threadIdx.y : threadIdx.x;
@@ -328,7 +331,113 @@ sweep_kernel(SweepArgs<R> a) {
 
         // ---- face f = fc + slot (between cells f and f+1): cell positions slot .. slot+5
         const int f = fc + slot;
-        if (CHAR == 0 && line_ok && f < fe) {
+        if constexpr (DIR == 0 && CHAR == 0 && INTERP == I_MDCD_HYBRID) {
+            // Along x a warp is one line and its lanes are consecutive faces.
+            // The detector at a face's right-hand centre (cell f+1) is the
+            // left-hand centre of the next face, so each lane evaluates one
+            // centre and takes the other from the lane before it (lane 0: from
+            // lane 31 of the previous chunk; in the first chunk it evaluates
+            // both).  Same values as evaluating both centres per face.
+            if (line_ok) {  // uniform over the warp
+                R st[5][6];
+#pragma unroll
+                for (int q = 0; q < 5; ++q)
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) st[q][m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
+                unsigned r3 = 0;  // bit q: the detector rejects the linear scheme at cell f+1
+#pragma unroll
+                for (int q = 0; q < 5; ++q)
+                    r3 |= (mdcd_smooth(st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]) ? 0u : 1u) << q;
+                unsigned r2 = __shfl_up_sync(0xffffffffu, r3, 1);
+                if (slot == 0) {
+                    if (fc == fb) {
+                        r2 = 0;
+#pragma unroll
+                        for (int q = 0; q < 5; ++q)
+                            r2 |= (mdcd_smooth(st[q][0], st[q][1], st[q][2], st[q][3], st[q][4]) ? 0u : 1u) << q;
+                    } else {
+                        r2 = det_carry;
+                    }
+                }
+                det_carry = __shfl_sync(0xffffffffu, r3, 31);
+                if (f < fe) {
+                    const unsigned weno = r2 | r3;
+                    R UL[5], UR[5];
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) {
+                        UL[q] = mdcd_linear(a.sp.lin, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]);
+                        UR[q] = mdcd_linear(a.sp.lin, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1], st[q][0]);
+                    }
+                    if (weno) {
+#pragma unroll
+                        for (int q = 0; q < 5; ++q)
+                            if (weno & (1u << q)) {
+                                UL[q] = mdcd_weno_branch(a.sp.hd, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4],
+                                                         st[q][5]);
+                                UR[q] = mdcd_weno_branch(a.sp.hd, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1],
+                                                         st[q][0]);
+                            }
+                    }
+                    R F[5];
+                    riemann<DIR, R, RS>(a.sp, UL, UR, F);
+                    const int s = G::template idx<NF>(line, slot + 5);
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) sF[q * NL * NF + s] = F[q];
+                }
+            }
+        } else if constexpr (DIR != 0 && CHAR == 0 && INTERP == I_MDCD_HYBRID) {
+            // Along y and z the faces of a line are spread over the warps:
+            // each face evaluates the detector at its right-hand centre (cell
+            // f+1) into shared memory and, after a barrier, reads its
+            // left-hand centre (cell f) written by the face before it.  Cell
+            // fc comes from the previous chunk's last face (moved with the
+            // tails); the first chunk's first face evaluates it.
+            const bool act = line_ok && f < fe;
+            R st[5][6];
+            unsigned r3 = 0;
+            if (act) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q)
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) st[q][m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
+#pragma unroll
+                for (int q = 0; q < 5; ++q)
+                    r3 |= (mdcd_smooth(st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]) ? 0u : 1u) << q;
+                sDet[(slot + 1) * NL + line] = (unsigned char)r3;
+                if (fc == fb && slot == 0) {
+                    unsigned r2 = 0;
+#pragma unroll
+                    for (int q = 0; q < 5; ++q)
+                        r2 |= (mdcd_smooth(st[q][0], st[q][1], st[q][2], st[q][3], st[q][4]) ? 0u : 1u) << q;
+                    sDet[line] = (unsigned char)r2;
+                }
+            }
+            __syncthreads();  // detector bits of this chunk's cells complete
+            if (act) {
+                const unsigned weno = r3 | sDet[slot * NL + line];
+                R UL[5], UR[5];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    UL[q] = mdcd_linear(a.sp.lin, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]);
+                    UR[q] = mdcd_linear(a.sp.lin, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1], st[q][0]);
+                }
+                if (weno) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q)
+                        if (weno & (1u << q)) {
+                            UL[q] = mdcd_weno_branch(a.sp.hd, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4],
+                                                     st[q][5]);
+                            UR[q] = mdcd_weno_branch(a.sp.hd, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1],
+                                                     st[q][0]);
+                        }
+                }
+                R F[5];
+                riemann<DIR, R, RS>(a.sp, UL, UR, F);
+                const int s = G::template idx<NF>(line, slot + 5);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) sF[q * NL * NF + s] = F[q];
+            }
+        } else if (CHAR == 0 && line_ok && f < fe) {
             R st[5][6];
 #pragma unroll
             for (int q = 0; q < 5; ++q)
@@ -385,6 +494,10 @@ sweep_kernel(SweepArgs<R> a) {
         }
         if constexpr (kRoldSmem) cp_async_wait<1>();  // this thread's old-RHS copies landed
         __syncthreads();  // faces of this chunk complete
+        if constexpr (DIR != 0 && CHAR == 0 && INTERP == I_MDCD_HYBRID) {
+            // the last face's bits (cell fc + C) become the next chunk's cell fc
+            if (line_ok && slot == C - 1) sDet[line] = sDet[C * NL + line];
+        }
         if constexpr (kRoldSmem) {
             if (rmw && upd) {
 #pragma unroll
