@@ -111,7 +111,7 @@ struct SweepGeom {
 // chunk's cells (true) or loaded into registers (false).
 constexpr bool kRoldSmem = true;
 // minimum resident blocks per SM requested from the register allocator
-template <typename R>
+template <int DIR, typename R>
 constexpr int sweep_min_blocks() { return 2; }
 
 // buffers U(5) F(5) V(4) [W(5) for characteristic bases], staging W(5)+V(4)
@@ -172,7 +172,7 @@ __device__ __forceinline__ void fused_stage_cell(const FusedStage &f, double dt,
 }
 
 template <int DIR, typename R, int INTERP, int RS, int CHAR>
-__global__ void __launch_bounds__(256, sweep_min_blocks<R>())
+__global__ void __launch_bounds__(256, sweep_min_blocks<DIR, R>())
 sweep_kernel(SweepArgs<R> a) {
     using G = SweepGeom<DIR>;
     constexpr int C = G::C, NL = G::NLINE, CH = G::CH, NU = G::NU, NF = G::NF, NV = G::NV;
@@ -339,43 +339,36 @@ sweep_kernel(SweepArgs<R> a) {
             // lane 31 of the previous chunk; in the first chunk it evaluates
             // both).  Same values as evaluating both centres per face.
             if (line_ok) {  // uniform over the warp
-                R st[5][6];
+                // one variable's stencil at a time (its registers die with it);
+                // the rare WENO branch re-reads its stencil from shared memory
+                R UL[5], UR[5];
+                unsigned r3 = 0, r2f = 0;  // bit q: the detector rejects the linear scheme at cell f+1 / f
 #pragma unroll
-                for (int q = 0; q < 5; ++q)
+                for (int q = 0; q < 5; ++q) {
+                    R sq[6];
 #pragma unroll
-                    for (int m = 0; m < 6; ++m) st[q][m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
-                unsigned r3 = 0;  // bit q: the detector rejects the linear scheme at cell f+1
-#pragma unroll
-                for (int q = 0; q < 5; ++q)
-                    r3 |= (mdcd_smooth(st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]) ? 0u : 1u) << q;
-                unsigned r2 = __shfl_up_sync(0xffffffffu, r3, 1);
-                if (slot == 0) {
-                    if (fc == fb) {
-                        r2 = 0;
-#pragma unroll
-                        for (int q = 0; q < 5; ++q)
-                            r2 |= (mdcd_smooth(st[q][0], st[q][1], st[q][2], st[q][3], st[q][4]) ? 0u : 1u) << q;
-                    } else {
-                        r2 = det_carry;
-                    }
+                    for (int m = 0; m < 6; ++m) sq[m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
+                    r3 |= (mdcd_smooth(sq[1], sq[2], sq[3], sq[4], sq[5]) ? 0u : 1u) << q;
+                    if (fc == fb && slot == 0)
+                        r2f |= (mdcd_smooth(sq[0], sq[1], sq[2], sq[3], sq[4]) ? 0u : 1u) << q;
+                    UL[q] = mdcd_linear(a.sp.lin, sq[0], sq[1], sq[2], sq[3], sq[4], sq[5]);
+                    UR[q] = mdcd_linear(a.sp.lin, sq[5], sq[4], sq[3], sq[2], sq[1], sq[0]);
                 }
+                unsigned r2 = __shfl_up_sync(0xffffffffu, r3, 1);
+                if (slot == 0) r2 = fc == fb ? r2f : det_carry;
                 det_carry = __shfl_sync(0xffffffffu, r3, 31);
                 if (f < fe) {
                     const unsigned weno = r2 | r3;
-                    R UL[5], UR[5];
-#pragma unroll
-                    for (int q = 0; q < 5; ++q) {
-                        UL[q] = mdcd_linear(a.sp.lin, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]);
-                        UR[q] = mdcd_linear(a.sp.lin, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1], st[q][0]);
-                    }
                     if (weno) {
 #pragma unroll
                         for (int q = 0; q < 5; ++q)
                             if (weno & (1u << q)) {
-                                UL[q] = mdcd_weno_branch(a.sp.hd, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4],
-                                                         st[q][5]);
-                                UR[q] = mdcd_weno_branch(a.sp.hd, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1],
-                                                         st[q][0]);
+                                const volatile R *vq = sU + q * NL * NU;
+                                R sq[6];
+#pragma unroll
+                                for (int m = 0; m < 6; ++m) sq[m] = vq[G::template idx<NU>(line, slot + m)];
+                                UL[q] = mdcd_weno_branch(a.sp.hd, sq[0], sq[1], sq[2], sq[3], sq[4], sq[5]);
+                                UR[q] = mdcd_weno_branch(a.sp.hd, sq[5], sq[4], sq[3], sq[2], sq[1], sq[0]);
                             }
                     }
                     R F[5];
@@ -393,42 +386,39 @@ sweep_kernel(SweepArgs<R> a) {
             // fc comes from the previous chunk's last face (moved with the
             // tails); the first chunk's first face evaluates it.
             const bool act = line_ok && f < fe;
-            R st[5][6];
+            // one variable's stencil at a time (its registers die with it);
+            // the rare WENO branch re-reads its stencil from shared memory
+            R UL[5], UR[5];
             unsigned r3 = 0;
             if (act) {
+                unsigned r2f = 0;
 #pragma unroll
-                for (int q = 0; q < 5; ++q)
+                for (int q = 0; q < 5; ++q) {
+                    R sq[6];
 #pragma unroll
-                    for (int m = 0; m < 6; ++m) st[q][m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
-#pragma unroll
-                for (int q = 0; q < 5; ++q)
-                    r3 |= (mdcd_smooth(st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]) ? 0u : 1u) << q;
-                sDet[(slot + 1) * NL + line] = (unsigned char)r3;
-                if (fc == fb && slot == 0) {
-                    unsigned r2 = 0;
-#pragma unroll
-                    for (int q = 0; q < 5; ++q)
-                        r2 |= (mdcd_smooth(st[q][0], st[q][1], st[q][2], st[q][3], st[q][4]) ? 0u : 1u) << q;
-                    sDet[line] = (unsigned char)r2;
+                    for (int m = 0; m < 6; ++m) sq[m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
+                    r3 |= (mdcd_smooth(sq[1], sq[2], sq[3], sq[4], sq[5]) ? 0u : 1u) << q;
+                    if (fc == fb && slot == 0)
+                        r2f |= (mdcd_smooth(sq[0], sq[1], sq[2], sq[3], sq[4]) ? 0u : 1u) << q;
+                    UL[q] = mdcd_linear(a.sp.lin, sq[0], sq[1], sq[2], sq[3], sq[4], sq[5]);
+                    UR[q] = mdcd_linear(a.sp.lin, sq[5], sq[4], sq[3], sq[2], sq[1], sq[0]);
                 }
+                sDet[(slot + 1) * NL + line] = (unsigned char)r3;
+                if (fc == fb && slot == 0) sDet[line] = (unsigned char)r2f;
             }
             __syncthreads();  // detector bits of this chunk's cells complete
             if (act) {
                 const unsigned weno = r3 | sDet[slot * NL + line];
-                R UL[5], UR[5];
-#pragma unroll
-                for (int q = 0; q < 5; ++q) {
-                    UL[q] = mdcd_linear(a.sp.lin, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4], st[q][5]);
-                    UR[q] = mdcd_linear(a.sp.lin, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1], st[q][0]);
-                }
                 if (weno) {
 #pragma unroll
                     for (int q = 0; q < 5; ++q)
                         if (weno & (1u << q)) {
-                            UL[q] = mdcd_weno_branch(a.sp.hd, st[q][0], st[q][1], st[q][2], st[q][3], st[q][4],
-                                                     st[q][5]);
-                            UR[q] = mdcd_weno_branch(a.sp.hd, st[q][5], st[q][4], st[q][3], st[q][2], st[q][1],
-                                                     st[q][0]);
+                            const volatile R *vq = sU + q * NL * NU;
+                            R sq[6];
+#pragma unroll
+                            for (int m = 0; m < 6; ++m) sq[m] = vq[G::template idx<NU>(line, slot + m)];
+                            UL[q] = mdcd_weno_branch(a.sp.hd, sq[0], sq[1], sq[2], sq[3], sq[4], sq[5]);
+                            UR[q] = mdcd_weno_branch(a.sp.hd, sq[5], sq[4], sq[3], sq[2], sq[1], sq[0]);
                         }
                 }
                 R F[5];
