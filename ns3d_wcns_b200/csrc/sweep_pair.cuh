@@ -10,8 +10,8 @@
 //   * every shared-memory access moves a 64-bit word (both lines at once), and
 //   * along y and z the two lines are x-neighbours, so the global loads,
 //     stores and cp.async copies are 8 bytes (16 for the FP64 state).
-// The Riemann solvers and the rare WENO branch of the hybrid scheme run per
-// line on the unpacked halves.  The arithmetic of each half is the scalar
+// HLLC runs paired too (hllc_flux2); the other Riemann solvers and the rare
+// WENO branch of the hybrid scheme run per line on the unpacked halves.  The arithmetic of each half is the scalar
 // kernel's; only the placement of fused multiply-adds differs, so results
 // agree with it to FP32 rounding (the mixed path has an accuracy bound, not
 // a bitwise contract).
@@ -75,6 +75,87 @@ __device__ __forceinline__ void mdcd_smooth2(float2 fm2, float2 fm1, float2 f0, 
     const float2 rhs = mul2(p2(0.4f), add2(fma2(A, A, mul2(B, B)), p2(eps)));
     sa = lhs.x > rhs.x;
     sb = lhs.y > rhs.y;
+}
+
+// hllc_flux (HLLC_Riemann_solver, InviscousFlux.cpp:449-592) for both lines:
+// the side states, wave speeds, S_M and the star flux of the upwind side in
+// paired arithmetic; reciprocals, square roots, divisions, minima and the
+// side selection per half.  Faces with S_L >= 0 or S_R <= 0 (supersonic,
+// rare) and S_M denominators below 1e-12 take the scalar forms per half.
+template <int DIR>
+__device__ __forceinline__ void hllc_flux2(const float2 *UL, const float2 *UR, float g, float2 *F) {
+    const float2 rL = UL[0], rR = UR[0], EL = UL[4], ER = UR[4];
+    const float2 irL = make_float2(1.f / rL.x, 1.f / rL.y), irR = make_float2(1.f / rR.x, 1.f / rR.y);
+    const float2 uL = mul2(UL[1], irL), vL = mul2(UL[2], irL), wL = mul2(UL[3], irL);
+    const float2 uR = mul2(UR[1], irR), vR = mul2(UR[2], irR), wR = mul2(UR[3], irR);
+    const float2 gm1 = p2(g - 1.f), mh = p2(-0.5f);
+    const float2 pL = mul2(fma2(mul2(mh, rL), fma2(wL, wL, fma2(vL, vL, mul2(uL, uL))), EL), gm1);
+    const float2 pR = mul2(fma2(mul2(mh, rR), fma2(wR, wR, fma2(vR, vR, mul2(uR, uR))), ER), gm1);
+    const float2 unL = DIR == 0 ? uL : (DIR == 1 ? vL : wL), unR = DIR == 0 ? uR : (DIR == 1 ? vR : wR);
+    const float2 tL = mul2(mul2(p2(g), pL), irL), tR = mul2(mul2(p2(g), pR), irR);
+    const float2 aL = make_float2(sqrtf(tL.x), sqrtf(tL.y)), aR = make_float2(sqrtf(tR.x), sqrtf(tR.y));
+    const float2 dL = sub2(unL, aL), dR = sub2(unR, aR), eL = add2(unL, aL), eR = add2(unR, aR);
+    const float2 SL = make_float2(fminf(dL.x, dR.x), fminf(dL.y, dR.y));
+    const float2 SR = make_float2(fmaxf(eL.x, eR.x), fmaxf(eL.y, eR.y));
+    const float2 cR = sub2(SR, unR), cL = sub2(SL, unL);
+    const float2 num = add2(sub2(mul2(mul2(rR, unR), cR), mul2(mul2(rL, unL), cL)), sub2(pL, pR));
+    const float2 den = sub2(mul2(rR, cR), mul2(rL, cL));
+    float2 SM;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const float n_ = h ? num.y : num.x, d_ = h ? den.y : den.x;
+        float sm;
+        if (fabsf(d_) > 1e-12f) {
+            sm = n_ / d_;
+        } else {
+            const float sL = sqrtf(h ? rL.y : rL.x), sR = sqrtf(h ? rR.y : rR.x);
+            sm = (sL * (h ? unL.y : unL.x) + sR * (h ? unR.y : unR.x)) / (sL + sR);
+        }
+        if (h) SM.y = sm; else SM.x = sm;
+    }
+    // the star state of the upwind side, per half
+    const bool lx = SM.x >= 0.f, ly = SM.y >= 0.f;
+    auto sel = [&](float2 l, float2 r) { return make_float2(lx ? l.x : r.x, ly ? l.y : r.y); };
+    const float2 r = sel(rL, rR), ir = sel(irL, irR), u = sel(uL, uR), v = sel(vL, vR), w = sel(wL, wR);
+    const float2 E = sel(EL, ER), p = sel(pL, pR), un = sel(unL, unR), Sk = sel(SL, SR);
+    const float2 U1 = sel(UL[1], UR[1]), U2 = sel(UL[2], UR[2]), U3 = sel(UL[3], UR[3]);
+    const float2 m = mul2(r, un);
+    const float2 zero = p2(0.f);
+    const float2 Fs0 = m;
+    const float2 Fs1 = fma2(m, u, DIR == 0 ? p : zero);
+    const float2 Fs2 = fma2(m, v, DIR == 1 ? p : zero);
+    const float2 Fs3 = fma2(m, w, DIR == 2 ? p : zero);
+    const float2 Fs4 = mul2(add2(E, p), un);
+    const float2 dk = sub2(Sk, un), rdk = mul2(r, dk), dS = sub2(Sk, SM);
+    const float2 rs = make_float2(rdk.x / dS.x, rdk.y / dS.y);
+    const float2 pr = make_float2(p.x / rdk.x, p.y / rdk.y);
+    const float2 Es = fma2(sub2(SM, un), add2(SM, pr), mul2(E, ir));
+    const float2 us = DIR == 0 ? SM : u, vs = DIR == 1 ? SM : v, ws = DIR == 2 ? SM : w;
+    F[0] = fma2(Sk, sub2(rs, r), Fs0);
+    F[1] = fma2(Sk, sub2(mul2(rs, us), U1), Fs1);
+    F[2] = fma2(Sk, sub2(mul2(rs, vs), U2), Fs2);
+    F[3] = fma2(Sk, sub2(mul2(rs, ws), U3), Fs3);
+    F[4] = fma2(Sk, sub2(mul2(rs, Es), E), Fs4);
+    // supersonic faces: the physical flux of the upwind state
+    if (SL.x >= 0.f || SR.x <= 0.f || SL.y >= 0.f || SR.y <= 0.f) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float sl = h ? SL.y : SL.x, sr = h ? SR.y : SR.x;
+            if (sl >= 0.f || sr <= 0.f) {
+                const float2 *Us = sl >= 0.f ? UL : UR;
+                float Uh[5], Fh[5];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) Uh[q] = h ? Us[q].y : Us[q].x;
+                Side<DIR, float> S;
+                S.load(Uh, g);
+                S.flux(Fh);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    if (h) F[q].y = Fh[q]; else F[q].x = Fh[q];
+                }
+            }
+        }
+    }
 }
 
 // Chunk geometry: C faces of NL = 2 NP lines per chunk, one thread per
@@ -322,14 +403,21 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
                     }
                 }
             }
-            float ULa[5], URa[5], ULb[5], URb[5], Fa[5], Fb[5];
-#pragma unroll
-            for (int q = 0; q < 5; ++q) { ULa[q] = UL[q].x; URa[q] = UR[q].x; ULb[q] = UL[q].y; URb[q] = UR[q].y; }
-            riemann<DIR, float, RS>(a.sp, ULa, URa, Fa);
-            riemann<DIR, float, RS>(a.sp, ULb, URb, Fb);
             const int s = G::template idx<NF>(pr, slot + 5);
+            if constexpr (RS == R_HLLC) {
+                float2 F[5];
+                hllc_flux2<DIR>(UL, UR, a.sp.gamma, F);
 #pragma unroll
-            for (int q = 0; q < 5; ++q) sF[q * NP * NF + s] = make_float2(Fa[q], Fb[q]);
+                for (int q = 0; q < 5; ++q) sF[q * NP * NF + s] = F[q];
+            } else {
+                float ULa[5], URa[5], ULb[5], URb[5], Fa[5], Fb[5];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) { ULa[q] = UL[q].x; URa[q] = UR[q].x; ULb[q] = UL[q].y; URb[q] = UR[q].y; }
+                riemann<DIR, float, RS>(a.sp, ULa, URa, Fa);
+                riemann<DIR, float, RS>(a.sp, ULb, URb, Fb);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) sF[q * NP * NF + s] = make_float2(Fa[q], Fb[q]);
+            }
         }
         cp_async_wait<1>();  // this thread's old-RHS / FP64-state copies landed
         __syncthreads();     // faces of this chunk complete
