@@ -66,7 +66,7 @@ __device__ __forceinline__ R sutherland(R mu0, R S, R T) {
     return mu0 * (T * sqrt(T)) * (R(1) + S) / (T + S);
 }
 
-constexpr int VTX = 32, VTY = 8, VH = NG, VZC = 16;
+constexpr int VTX = 32, VTY = 8, VH = NG, VZC = 32;
 
 // First derivative of the window value f(o), o in [-3, 3], with a block-
 // uniform order; the offsets stay compile-time so the window lives in
