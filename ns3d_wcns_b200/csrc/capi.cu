@@ -435,7 +435,10 @@ int rhs_impl(ns3d_handle *h, const FusedStage *fs = nullptr) {
         for (int q = 0; q < 3; ++q) maps.m[q] = sizeof(R) == 8 ? h->tmW64[h->s0][q] : h->tmW32[q];
         maps.m[3] = sizeof(R) == 8 ? h->tmT64 : h->tmT32;
         prof_begin(h, "viscous_flux");
-        viscous_flux_kernel<R><<<g, dim3(VTX, VTY), 0, st>>>(va, maps);
+        if (va.periodic[0] && va.periodic[1] && va.periodic[2])
+            viscous_flux_kernel<R, true><<<g, dim3(VTX, VTY), 0, st>>>(va, maps);
+        else
+            viscous_flux_kernel<R, false><<<g, dim3(VTX, VTY), 0, st>>>(va, maps);
         prof_end(h);
         h->launches += 1;
         CK(h, cudaGetLastError(), "viscous kernel");

@@ -115,7 +115,10 @@ constexpr int vtile_stride() {  // elements per tile, 128-byte aligned tiles
     return (int)(((VBX * VBY * sizeof(R) + 127) / 128) * 128 / sizeof(R));
 }
 
-template <typename R>
+// P6: every direction periodic, so every derivative is the 6th-order central
+// one (choose_scheme's order for periodic directions) and the order dispatch
+// compiles away.
+template <typename R, bool P6>
 __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, const __grid_constant__ ViscMaps tm) {
     constexpr int TS = vtile_stride<R>();
     __shared__ __align__(128) R sm[2 * 4 * TS];  // two plane tiles of u, v, w, T
@@ -130,8 +133,8 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
     const R *src[4] = {a.W[1], a.W[2], a.W[3], a.T};
     const long zs = (long)L.px * L.sy;
     const long col = L.at(min(i, L.nx - 1) + NG, min(j, L.ny - 1) + NG, 0);  // ghost-inclusive plane 0
-    const int ox = visc_order(i, L.nx, a.periodic[0]);
-    const int oy = visc_order(j, L.ny, a.periodic[1]);
+    const int ox = P6 ? 6 : visc_order(i, L.nx, a.periodic[0]);
+    const int oy = P6 ? 6 : visc_order(j, L.ny, a.periodic[1]);
     const int cx = threadIdx.x + VH + 1, cy = threadIdx.y + VH;
     auto tile = [&](int buf, int q) { return sm + (buf * 4 + q) * TS; };
     if (tid == 0) {
@@ -178,7 +181,7 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
         if (in) {
             const R *tu = tile(buf, 0), *tv = tile(buf, 1), *tw = tile(buf, 2), *tT = tile(buf, 3);
             const R *tq[4] = {tu, tv, tw, tT};
-            const int oz = visc_order(k, L.nz, a.periodic[2]);
+            const int oz = P6 ? 6 : visc_order(k, L.nz, a.periodic[2]);
             R g[4][3];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
