@@ -40,6 +40,11 @@ __device__ __forceinline__ void cp_async8(float2 *smem_dst, const float *gsrc) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
+// 16-byte copy of two float2 (four neighbouring lines), bypassing L1
+__device__ __forceinline__ void cp_async16f(float2 *smem_dst, const float *gsrc) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void cp_async16(double2 *smem_dst, const double *gsrc) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
@@ -250,6 +255,14 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
     const int chunk_end = n + NG + 2;
     const int ti = G::tidx(pr, slot);
     const float gm1 = a.sp.gamma - 1.f;
+    // z with nx a multiple of 4: the even pair copies its own and the next
+    // pair's values (four x-neighbouring lines, 16 bytes, past L1); the two
+    // pairs share line_ok and every staging condition.  The z-sweep's 111 KB
+    // of shared memory per block leave little L1 for 8-byte cp.async.ca
+    // copies (0.81 -> 0.69 ms at 256^3); along y, with a large L1, the
+    // 8-byte copies are faster (0.43 against 0.47 ms).
+    const bool wide = DIR == 2 && (L.nx & 3) == 0;
+    const bool lead = !wide || (pr & 1) == 0;
 
     auto wrap = [&](int c) { return per ? (c < NG ? c + n : (c >= n + NG ? c - n : c)) : c; };
     auto vis_pos = [&](int c) -> int {
@@ -265,6 +278,10 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
     auto cp2 = [&](float2 *dst, const float *src, long off) {
         if (DIR == 0) { cp_async(&dst->x, src); cp_async(&dst->y, src + off); }
         else cp_async8(dst, src);
+    };
+    auto cpw = [&](float2 *dst, const float *src, long off) {
+        if (wide) { if (lead) cp_async16f(dst, src); }
+        else cp2(dst, src, off);
     };
     auto st2 = [&](float *p, long off, float2 v) {
         if (DIR == 0) { p[0] = v.x; p[off] = v.y; }
@@ -318,7 +335,7 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
         const long cid = lbase + cu * lstride;
         if (rmw && upd) {
 #pragma unroll
-            for (int q = 0; q < 5; ++q) cp2(&srold[q * CH + ti], a.Rhs[q] + cid, lpair);
+            for (int q = 0; q < 5; ++q) cpw(&srold[q * CH + ti], a.Rhs[q] + cid, lpair);
         }
         if constexpr (DIR == 2) {
             if (a.fs.stage && upd) {  // the FP64 state of the two cells this thread updates
@@ -338,12 +355,12 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
         if (stage) {
             const long id = lbase + wrap(cn) * lstride;
 #pragma unroll
-            for (int q = 0; q < 5; ++q) cp2(&stg[q * CH + ti], a.W[q] + id, lpair);
+            for (int q = 0; q < 5; ++q) cpw(&stg[q * CH + ti], a.W[q] + id, lpair);
             if (visc) {
                 const int ci = vis_pos(cn);
                 if (ci >= 0) {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) cp2(&stg[(5 + q) * CH + ti], a.V[q] + vbase + ci * vstride, vpair);
+                    for (int q = 0; q < 4; ++q) cpw(&stg[(5 + q) * CH + ti], a.V[q] + vbase + ci * vstride, vpair);
                 } else {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) stg[(5 + q) * CH + ti] = p2(0.f);

@@ -91,3 +91,15 @@ def test_pair_vs_scalar_fused_steps(gpu_lib, monkeypatch):
     for q in range(5):
         assert analysis.rel_l2(out[False][0][q], out[True][0][q]) <= 1e-5, q
     assert abs(out[False][1] / out[True][1] - 1) <= 1e-6
+
+
+def test_pair_narrow_copies(gpu_lib, monkeypatch):
+    """nx even but not a multiple of 4: the z sweep stays paired with 8-byte
+    copies per pair (its 16-byte copies need four aligned lines)."""
+    n = (18, 20, 16)
+    P, G = make_params(n=n, L=(1.0, 1.0, 1.0), interpolation=2, riemann=2, Re=300.0, precision=1)
+    st = random_state(n, seed=4)
+    a = _rhs(P, G, st, False, monkeypatch)
+    b = _rhs(P, G, st, True, monkeypatch)
+    for q in range(5):
+        assert analysis.rel_l2(a[q], b[q]) <= CONT_TOL
