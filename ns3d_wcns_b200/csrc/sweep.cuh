@@ -121,7 +121,7 @@ constexpr size_t sweep_smem_bytes() {
     using G = SweepGeom<DIR>;
     return sizeof(R) * ((size_t)G::NLINE * (5 * G::NU + 5 * G::NF + 4 * G::NV + (CHARW ? 5 * G::NU : 0)) +
                         (size_t)(kRoldSmem ? 14 : 9) * G::CH) +
-           ((DIR == 2 && sizeof(R) == 4) ? (size_t)10 * G::CH * sizeof(double) : 0);  // mixed fused stage: U0, Uc
+           (DIR == 2 ? (size_t)(sizeof(R) == 4 ? 10 : 5) * G::CH * sizeof(double) : 0);  // fused stage staging
 }
 
 template <typename R>
@@ -148,10 +148,19 @@ __device__ __forceinline__ R dstencil_inv(F f, int order, const R *dinv) {
 // Stage update of interior cell c (padded FP64 index) from its final
 // right-hand side r and current conserved state Uc (the sweep's exact p2c of
 // W): the operations of stage_kernel64 for an interior cell, so the same bits.
+// w0: the cell's step-start primitives (staged by the sweep; stages 2 and 3
+// only -- in stage 1 the step-start state is the current one, whose exact p2c
+// the sweep already holds).
 __device__ __forceinline__ void fused_stage_cell(const FusedStage &f, double dt, long c, const double *r,
-                                                 const double *Ucur, double &smax, double &ke, double &kc) {
+                                                 const double *Ucur, const double *w0, double &smax, double &ke,
+                                                 double &kc) {
     double U0[5], U[5], W[5];
-    p2c_exact(f.W0[0][c], f.W0[1][c], f.W0[2][c], f.W0[3][c], f.W0[4][c], f.gamma, U0);
+    if (f.stage == 1) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) U0[q] = Ucur[q];
+    } else {
+        p2c_exact(w0[0], w0[1], w0[2], w0[3], w0[4], f.gamma, U0);
+    }
 #pragma unroll
     for (int q = 0; q < 5; ++q) U[q] = rk_combine(f.stage, U0[q], f.stage == 1 ? U0[q] : Ucur[q], r[q], dt);
     c2p_exact(U, f.gamma, W);
@@ -185,7 +194,7 @@ sweep_kernel(SweepArgs<R> a) {
     R *const stg = sW + (USE_W ? 5 * NL * NU : 0);   // [9][CH]
     R *const srold = stg + 9 * CH;                   // [5][CH] (kRoldSmem)
     // mixed fused stage (float z-sweep only): staged FP64 U0 (rows 0-4), Uc (5-9)
-    double *const sUf = reinterpret_cast<double *>(srold + 5 * CH);
+    double *const sUf = reinterpret_cast<double *>(srold + 5 * CH);  // z fused stage: [10][CH] / [5][CH] FP64
 
     if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
@@ -294,6 +303,12 @@ sweep_kernel(SweepArgs<R> a) {
             } else {
 #pragma unroll
                 for (int q = 0; q < 5; ++q) rold[q] = a.Rhs[q][cid];
+            }
+        }
+        if constexpr (DIR == 2 && sizeof(R) == 8) {
+            if (a.fs.stage > 1 && upd) {  // the step-start primitives of the cell this thread updates
+#pragma unroll
+                for (int q = 0; q < 5; ++q) cp_async(&sUf[q * CH + ti], a.fs.W0[q] + cid);
             }
         }
         if constexpr (DIR == 2 && sizeof(R) == 4) {
@@ -562,7 +577,10 @@ sweep_kernel(SweepArgs<R> a) {
                         Uc[q] = sU[q * NL * NU + G::template idx<NU>(line, slot)];
                         rr[q] = rq[q];
                     }
-                    fused_stage_cell(a.fs, fdt, cid, rr, Uc, cfl_acc, ke_acc, ke_c);
+                    double w0[5];
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) w0[q] = a.fs.stage > 1 ? sUf[q * CH + ti] : 0.0;
+                    fused_stage_cell(a.fs, fdt, cid, rr, Uc, w0, cfl_acc, ke_acc, ke_c);
                     fused = true;
                 }
             }
