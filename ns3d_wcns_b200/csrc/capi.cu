@@ -877,6 +877,7 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     if (cudaSetDevice(h->device) != cudaSuccess) { delete h; return NS3D_ERR_NO_DEVICE; }
     h->L64 = make_layout<double>(grid->nx, grid->ny, grid->nz);
     h->L32 = make_layout<float>(grid->nx, grid->ny, grid->nz);
+    if (ghost_count(h->L64) >= (1L << 31)) { delete h; return NS3D_ERR_SIZE; }  // 32-bit ghost decode
     // derived constants, initialization.cpp:170-172, 194-197
     Phys &ph = h->ph;
     ph.gamma = params->gamma;

@@ -196,28 +196,32 @@ __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel_mixed(StageArgsMix
 // Ghost cells only, one thread each: t enumerates the two z-slabs (full x-y
 // planes), then the y-slabs of the interior planes, then the x-ghosts of the
 // interior rows.
-__device__ __forceinline__ bool ghost_cell(const Layout &L, long t, int &i, int &j, int &k) {
-    const long gz = 6L * L.sy * L.sx, gy = 6L * L.nz * L.sx, gx = 6L * L.nz * L.ny;
+// Ghost cell number t: the two z-slabs (3 planes each, full sy x sx), then the
+// y-slabs of the interior planes, then the x-slabs of the interior rows.  The
+// decode runs in 32-bit unsigned arithmetic (the host checks ghost_count <
+// 2^31): 64-bit divisions are several times slower.
+__device__ __forceinline__ bool ghost_cell(const Layout &L, long t64, int &i, int &j, int &k) {
+    const unsigned sx = (unsigned)L.sx, sy = (unsigned)L.sy, nz = (unsigned)L.nz, ny = (unsigned)L.ny;
+    const unsigned gz = 6u * sy * sx, gy = 6u * nz * sx, gx = 6u * nz * ny;
+    if (t64 < 0 || t64 >= (long)gz + gy + gx) return false;
+    unsigned t = (unsigned)t64;
     if (t < gz) {
-        const long sl = t / ((long)L.sy * L.sx), rem = t % ((long)L.sy * L.sx);
-        k = sl < 3 ? (int)sl : L.nz + (int)sl; j = (int)(rem / L.sx); i = (int)(rem % L.sx);
+        const unsigned pl = sy * sx, sl = t / pl, rem = t - sl * pl, jj = rem / sx;
+        k = sl < 3 ? (int)sl : L.nz + (int)sl; j = (int)jj; i = (int)(rem - jj * sx);
         return true;
     }
     t -= gz;
     if (t < gy) {
-        k = (int)(t / (6L * L.sx)) + NG;
-        const long rem = t % (6L * L.sx), sl = rem / L.sx;
-        j = sl < 3 ? (int)sl : L.ny + (int)sl; i = (int)(rem % L.sx);
+        const unsigned rw = 6u * sx, kk = t / rw, rem = t - kk * rw, sl = rem / sx;
+        k = (int)kk + NG;
+        j = sl < 3 ? (int)sl : L.ny + (int)sl; i = (int)(rem - sl * sx);
         return true;
     }
     t -= gy;
-    if (t < gx) {
-        const long row = t / 6, sl = t % 6;
-        k = (int)(row / L.ny) + NG; j = (int)(row % L.ny) + NG;
-        i = sl < 3 ? (int)sl : L.nx + (int)sl;
-        return true;
-    }
-    return false;
+    const unsigned row = t / 6u, sl = t - row * 6u, kk = row / ny;
+    k = (int)kk + NG; j = (int)(row - kk * ny) + NG;
+    i = sl < 3 ? (int)sl : L.nx + (int)sl;
+    return true;
 }
 
 __host__ __device__ inline long ghost_count(const Layout &L) {

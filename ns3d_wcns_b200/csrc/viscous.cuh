@@ -158,6 +158,7 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
         for (int q = 0; q < 4; ++q) win[q][m] = src[q][col + (long)(kb + m) * zs];
 #pragma unroll
     for (int q = 0; q < 4; ++q) nxt[q] = src[q][col + (long)(kb + 6) * zs];
+#pragma unroll 7  // the window shift becomes register renaming (7 planes)
     for (int k = kb; k < ke; ++k) {
         const int buf = (k - kb) & 1;
         const bool more = k + 1 < ke;
