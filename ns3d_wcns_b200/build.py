@@ -62,7 +62,9 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
                     sys.stderr.write(r.stdout + r.stderr)
                 if r.returncode != 0:
                     raise RuntimeError(f"nvcc failed on {futs[f]}")
-    if jobs or not os.path.exists(LIB):
+    # relink when anything was compiled, the library is missing, or an object is newer than it (a
+    # previous link that failed leaves the old library behind)
+    if jobs or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         tmp = LIB + ".tmp"
         cmd = [nvcc] + ARCH + ["-shared", "-o", tmp] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)
