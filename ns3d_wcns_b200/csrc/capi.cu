@@ -505,17 +505,23 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
     return NS3D_OK;
 }
 
-// One RK stage: right-hand side and update.  Plain FP64 path: the update is
-// fused into the z-sweep (FusedStage) and a ghost kernel fills the ghost cells
-// -- the same bits as the separate stage kernel; mixed path: RHS then the
-// separate stage kernel.  src0 = step-start state, srcc = this stage's state
+// One RK stage: right-hand side and update, fused into the z-sweep
+// (FusedStage), then a ghost kernel for the ghost cells.  Plain FP64 path: the
+// same bits as the separate stage kernel.  Mixed path: increment form -- the
+// FP32 increments of stages 1 and 2 live in the state buffer that is free
+// during the step (neither src0 nor the step's result), and only stage 3
+// writes the FP64 state.  src0 = step-start state, srcc = this stage's state
 // (the sweeps read h->s0, which the caller has set to srcc), dst = new state.
 int rk_stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double dt) {
     if (h->mixed) {
+        // rk3_async's buffers: (1: s0, s0 -> b1), (2: s0, b1 -> b2), (3: s0, b2 -> b1)
+        const int free_buf = 3 - src0 - (stage == 2 ? srcc : dst);
+        if (free_buf < 0 || free_buf > 2 || free_buf == src0 || (stage != 2 && free_buf == dst)) return NS3D_ERR_STATE;
         FusedStage f{};
         f.stage = stage;
         for (int q = 0; q < 5; ++q) {
-            f.U0[q] = h->S[src0][q]; f.Uc[q] = h->S[srcc][q]; f.Uout[q] = h->S[dst][q];
+            f.U0[q] = h->S[src0][q]; f.Uout[q] = h->S[dst][q];
+            f.D[q] = reinterpret_cast<float *>(h->S[free_buf][q]);  // FP32 layout inside an FP64 plane
             f.W32out[q] = h->w32[q];  // in place (the sweep defers the cells its wrap re-reads)
         }
         f.T32out = h->T32;
@@ -531,8 +537,8 @@ int rk_stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, doubl
         if (r) return r;
         StageArgsMixed a;
         for (int q = 0; q < 5; ++q) {
-            a.U0[q] = h->S[src0][q]; a.Uc[q] = h->S[srcc][q]; a.Rhs[q] = h->rhs32[q];
-            a.Uout[q] = h->S[dst][q]; a.Wout[q] = h->w32[q];
+            a.U0[q] = h->S[src0][q]; a.Uc[q] = nullptr; a.Rhs[q] = h->rhs32[q];
+            a.Uout[q] = h->S[dst][q]; a.Wout[q] = h->w32[q]; a.D[q] = f.D[q];
         }
         a.L = h->L64; a.L32 = h->L32; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
         a.Tout = h->T32; a.Rgas = h->ph.Rgas;
@@ -878,6 +884,8 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     h->L64 = make_layout<double>(grid->nx, grid->ny, grid->nz);
     h->L32 = make_layout<float>(grid->nx, grid->ny, grid->nz);
     if (ghost_count(h->L64) >= (1L << 31)) { delete h; return NS3D_ERR_SIZE; }  // 32-bit ghost decode
+    // the mixed path's FP32 stage increments live inside an FP64 state plane
+    if ((size_t)h->L32.plane * 4 > (size_t)h->L64.plane * 8) { delete h; return NS3D_ERR_CONFIG; }
     // derived constants, initialization.cpp:170-172, 194-197
     Phys &ph = h->ph;
     ph.gamma = params->gamma;

@@ -130,6 +130,7 @@ struct StageArgsMixed {
     double dx, vol;
     const double *dt_dev;   // non-null: dt from the device time loop (replaces dt)
     const int *done;        // non-null: skip the launch while *done
+    const float *D[5];      // ghost kernel after the fused z-sweep: stage increments (FP32 layout)
 };
 
 __global__ void __launch_bounds__(STAGE_THREADS) stage_kernel_mixed(StageArgsMixed a) {
@@ -271,13 +272,19 @@ __global__ void __launch_bounds__(256) stage_ghost_kernel64(StageArgs64 a) {
     a.Tout[o] = W[4] / __dmul_rn(W[0], a.Rgas);
 }
 
+// Ghost cells after the mixed path's fused z-sweep (increment form, see
+// FusedStage): a ghost whose source is an interior cell gets that cell's new
+// state -- U0 + D after stages 1 and 2 (the conversion the sweep applies, so
+// the same FP32 primitives), the FP64 state after stage 3 -- with sign flips;
+// a ghost whose source is a ghost keeps its step-start state (its right-hand
+// side is zero in every stage); special states are constants.  Only stage 3
+// writes the FP64 state's ghosts.
 __global__ void __launch_bounds__(256) stage_ghost_kernel_mixed(StageArgsMixed a) {
     if (a.done && *a.done) return;
     const Layout &L = a.L;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     int i, j, k;
     if (!ghost_cell(L, t, i, j, k)) return;
-    const double dt = a.dt_dev ? *a.dt_dev : a.dt;
     int c[3] = {i, j, k};
     int flip;
     const int kind = resolve_source(L, a.b, c, flip);
@@ -290,17 +297,18 @@ __global__ void __launch_bounds__(256) stage_ghost_kernel_mixed(StageArgsMixed a
     } else {
         const long s = L.at(c[0], c[1], c[2]);
         if (is_interior(L, c)) {
+            if (a.stage == 3) {
 #pragma unroll
-            for (int q = 0; q < 5; ++q) U[q] = a.Uout[q][s];  // new value, already clamped
+                for (int q = 0; q < 5; ++q) U[q] = a.Uout[q][s];  // new value, already clamped
+            } else {
+                const long s32 = a.L32.at(c[0], c[1], c[2]);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) U[q] = a.U0[q][s] + (double)a.D[q][s32];
+                if (U[0] <= 0.0) U[0] = 1e-12;
+            }
         } else {
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                const double u0 = a.U0[q][s];
-                const double u = a.stage == 1 ? u0 : a.Uc[q][s];
-                U[q] = a.stage == 1 ? u0 + dt * 0.0
-                     : a.stage == 2 ? 0.75 * u0 + 0.25 * (u + dt * 0.0)
-                                    : (1.0 / 3.0) * u0 + (2.0 / 3.0) * (u + dt * 0.0);
-            }
+            for (int q = 0; q < 5; ++q) U[q] = a.U0[q][s];
             if (U[0] <= 0.0) U[0] = 1e-12;
         }
         if (flip & 1) U[1] = -U[1];
@@ -308,13 +316,15 @@ __global__ void __launch_bounds__(256) stage_ghost_kernel_mixed(StageArgsMixed a
         if (flip & 4) U[3] = -U[3];
         c2p_fast(U, a.gamma, W, ir);  // the conversion the fused z-sweep gives the interior cells
     }
-    const long o = L.at(i, j, k);
+    if (a.stage == 3) {
+        const long o = L.at(i, j, k);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) a.Uout[q][o] = U[q];
+        for (int q = 0; q < 5; ++q) a.Uout[q][o] = U[q];
+    }
     const long o32 = a.L32.at(i, j, k);
 #pragma unroll
     for (int q = 0; q < 5; ++q) a.Wout[q][o32] = (float)W[q];
-    a.Tout[o32] = (float)(W[4] * ir / a.Rgas);
+    a.Tout[o32] = (float)(W[4] * ir * (1.0 / a.Rgas));  // as the z-sweep
 }
 
 }  // namespace ns3d

@@ -43,17 +43,20 @@ namespace ns3d {
 //   plain FP64 path: W0 -> Wout, Tout; the current conserved state is the
 //     sweep's exact p2c of W (shared buffer), so the bits equal the separate
 //     stage kernel's;
-//   mixed path: FP64 conserved U0 / Uc (staged with cp.async) -> Uout, and
-//     the FP32 primitives / temperature rewritten in place (W32out, T32out):
-//     the first five cells of a periodic line are re-read by its wrapped end,
-//     so their new primitives are written after the line.
+//   mixed path, in increment form: the FP64 step-start state U0 and the FP32
+//     stage increment D (both staged with cp.async) give U_s = U0 + D_s;
+//     stages 1 and 2 store the next increment (D_1 = dt L0, D_2 = (D_1 +
+//     dt L1) / 4) in D, stage 3 the FP64 state U0 + 2/3 (D_2 + dt L2) in
+//     Uout.  The FP32 primitives / temperature of U_s are rewritten in place
+//     (W32out, T32out): the first five cells of a periodic line are re-read
+//     by its wrapped end, so their new primitives are written after the line.
 struct FusedStage {
     int stage;
     const double *W0[5];
     double *Wout[5];
     double *Tout;
     const double *U0[5];
-    const double *Uc[5];
+    float *D[5];            // mixed: stage increments (FP32 layout), read and rewritten
     double *Uout[5];
     float *W32out[5];
     float *T32out;
@@ -121,7 +124,7 @@ constexpr size_t sweep_smem_bytes() {
     using G = SweepGeom<DIR>;
     return sizeof(R) * ((size_t)G::NLINE * (5 * G::NU + 5 * G::NF + 4 * G::NV + (CHARW ? 5 * G::NU : 0)) +
                         (size_t)(kRoldSmem ? 14 : 9) * G::CH) +
-           (DIR == 2 ? (size_t)(sizeof(R) == 4 ? 10 : 5) * G::CH * sizeof(double) : 0);  // fused stage staging
+           (DIR == 2 ? (size_t)5 * G::CH * (sizeof(double) + (sizeof(R) == 4 ? sizeof(float) : 0)) : 0);  // fused stage
 }
 
 template <typename R>
@@ -193,8 +196,9 @@ sweep_kernel(SweepArgs<R> a) {
     R *const sW = sV + 4 * NL * NV;                  // [5][NL*NU] characteristic bases only
     R *const stg = sW + (USE_W ? 5 * NL * NU : 0);   // [9][CH]
     R *const srold = stg + 9 * CH;                   // [5][CH] (kRoldSmem)
-    // mixed fused stage (float z-sweep only): staged FP64 U0 (rows 0-4), Uc (5-9)
-    double *const sUf = reinterpret_cast<double *>(srold + 5 * CH);  // z fused stage: [10][CH] / [5][CH] FP64
+    // fused stage (z-sweep): staged FP64 step-start state, and (mixed) the FP32 increment
+    double *const sUf = reinterpret_cast<double *>(srold + 5 * CH);  // z fused stage: [5][CH] FP64
+    float *const sDs = reinterpret_cast<float *>(sUf + 5 * CH);       // mixed: [5][CH] stage increment
 
     if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
@@ -318,7 +322,7 @@ sweep_kernel(SweepArgs<R> a) {
                 for (int q = 0; q < 5; ++q) cp_async(&sUf[q * CH + ti], a.fs.U0[q] + c64);
                 if (a.fs.stage > 1) {
 #pragma unroll
-                    for (int q = 0; q < 5; ++q) cp_async(&sUf[(5 + q) * CH + ti], a.fs.Uc[q] + c64);
+                    for (int q = 0; q < 5; ++q) cp_async(&sDs[q * CH + ti], a.fs.D[q] + cid);
                 }
             }
         }
@@ -592,17 +596,23 @@ sweep_kernel(SweepArgs<R> a) {
                     for (int q = 0; q < 5; ++q) {
                         const double rr = (double)rq[q];
                         const double u0 = sUf[q * CH + ti];
-                        const double u = f.stage == 1 ? u0 : sUf[(5 + q) * CH + ti];
-                        U[q] = f.stage == 1 ? u0 + fdt * rr
-                             : f.stage == 2 ? 0.75 * u0 + 0.25 * (u + fdt * rr)
-                                            : (1.0 / 3.0) * u0 + (2.0 / 3.0) * (u + fdt * rr);
+                        const double dp = f.stage == 1 ? 0.0 : (double)sDs[q * CH + ti];
+                        if (f.stage == 3) {
+                            U[q] = u0 + (2.0 / 3.0) * (dp + fdt * rr);
+                        } else {
+                            const float dn = (float)(f.stage == 1 ? fdt * rr : 0.25 * (dp + fdt * rr));
+                            f.D[q][cid] = dn;
+                            U[q] = u0 + (double)dn;
+                        }
                     }
                     if (U[0] <= 0.0) U[0] = 1e-12;
                     double W[5], ir;
                     c2p_fast(U, f.gamma, W, ir);
-                    const long c64 = f.L64.at(ta0 + NG, tb0 + NG, cu);
+                    if (f.stage == 3) {
+                        const long c64 = f.L64.at(ta0 + NG, tb0 + NG, cu);
 #pragma unroll
-                    for (int q = 0; q < 5; ++q) f.Uout[q][c64] = U[q];
+                        for (int q = 0; q < 5; ++q) f.Uout[q][c64] = U[q];
+                    }
                     if (per && cu < NG + 5) {  // re-read by the line's wrapped end: write after the line
                         has_def = true; def_id = cid;
 #pragma unroll

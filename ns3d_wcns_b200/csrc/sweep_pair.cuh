@@ -189,13 +189,13 @@ struct PairGeom {
 static_assert(PairGeom<2>::NL == SweepGeom<2>::NLINE, "the fused stage's CFL partials assume one z-sweep grid");
 
 // float2 units: U(5) F(5) V(4), staging W(5)+V(4), old RHS(5); z-sweep:
-// FP64 U0, Uc (10 double2) and the deferred primitives of the first five
-// cells of periodic lines (6 x 5 x NP float2)
+// FP64 U0 (5 double2), the FP32 stage increments (5 float2) and the deferred
+// primitives of the first five cells of periodic lines (6 x 5 x NP float2)
 template <int DIR>
 constexpr size_t pair_smem_bytes() {
     using G = PairGeom<DIR>;
     return 8 * ((size_t)G::NP * (5 * G::NU + 5 * G::NF + 4 * G::NV) + (size_t)14 * G::CH) +
-           (DIR == 2 ? (size_t)10 * G::CH * 16 + (size_t)6 * 5 * G::NP * 8 : 0);
+           (DIR == 2 ? (size_t)5 * G::CH * 16 + (size_t)5 * G::CH * 8 + (size_t)6 * 5 * G::NP * 8 : 0);
 }
 static_assert((PairGeom<2>::NP * (5 * PairGeom<2>::NU + 5 * PairGeom<2>::NF + 4 * PairGeom<2>::NV) +
                14 * PairGeom<2>::CH) % 2 == 0, "double2 staging must start 16-byte aligned");
@@ -219,8 +219,9 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
     float2 *const sV = sF + 5 * NP * NF;                       // [4][NP*NV]
     float2 *const stg = sV + 4 * NP * NV;                      // [9][CH]
     float2 *const srold = stg + 9 * CH;                        // [5][CH]
-    double2 *const sUf = reinterpret_cast<double2 *>(srold + 5 * CH);  // [10][CH] z: U0, Uc
-    float2 *const sDef = reinterpret_cast<float2 *>(sUf + 10 * CH);    // [6][5][NP] z: deferred W, T
+    double2 *const sUf = reinterpret_cast<double2 *>(srold + 5 * CH);  // [5][CH] z: U0
+    float2 *const sDs = reinterpret_cast<float2 *>(sUf + 5 * CH);      // [5][CH] z: stage increment
+    float2 *const sDef = sDs + 5 * CH;                                 // [6][5][NP] z: deferred W, T
 
     if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
                 for (int q = 0; q < 5; ++q) cp_async16(&sUf[q * CH + ti], a.fs.U0[q] + c64);
                 if (a.fs.stage > 1) {
 #pragma unroll
-                    for (int q = 0; q < 5; ++q) cp_async16(&sUf[(5 + q) * CH + ti], a.fs.Uc[q] + c64);
+                    for (int q = 0; q < 5; ++q) cpw(&sDs[q * CH + ti], a.fs.D[q] + cid, lpair);
                 }
             }
         }
@@ -512,11 +513,14 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
             bool fused = false;
             if constexpr (DIR == 2) {
                 if (a.fs.stage) {
-                    // runge_kutta_3's update of both cells in FP64 (range_kutta.cpp:53-91)
+                    // runge_kutta_3's update of both cells (range_kutta.cpp:53-91) in
+                    // increment form: U_s = U0 + D_s with the FP32 increments
+                    // D_1 = dt L0 and D_2 = (D_1 + dt L1) / 4 kept between stages,
+                    // and U_3 = U0 + 2/3 (D_2 + dt L2) in FP64
                     const FusedStage &fs = a.fs;
                     const long c64 = fs.L64.at(ta0 + NG, tb0 + NG, cu);
                     double2 Uo[5];
-                    float2 Wn[5], Tn;
+                    float2 Wn[5], Tn, Dn[5];
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         double U[5];
@@ -525,11 +529,15 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
                             const double rr = (double)(h ? rq[q].y : rq[q].x);
                             const double2 s0 = sUf[q * CH + ti];
                             const double u0 = h ? s0.y : s0.x;
-                            double u = u0;
-                            if (fs.stage > 1) { const double2 s1 = sUf[(5 + q) * CH + ti]; u = h ? s1.y : s1.x; }
-                            U[q] = fs.stage == 1 ? u0 + fdt * rr
-                                 : fs.stage == 2 ? 0.75 * u0 + 0.25 * (u + fdt * rr)
-                                                 : (1.0 / 3.0) * u0 + (2.0 / 3.0) * (u + fdt * rr);
+                            double dp = 0.0;
+                            if (fs.stage > 1) { const float2 d = sDs[q * CH + ti]; dp = (double)(h ? d.y : d.x); }
+                            if (fs.stage == 3) {
+                                U[q] = u0 + (2.0 / 3.0) * (dp + fdt * rr);
+                            } else {
+                                const float dn = (float)(fs.stage == 1 ? fdt * rr : 0.25 * (dp + fdt * rr));
+                                if (h) Dn[q].y = dn; else Dn[q].x = dn;
+                                U[q] = u0 + (double)dn;
+                            }
                         }
                         if (U[0] <= 0.0) U[0] = 1e-12;
                         double W[5], ir;
@@ -549,8 +557,13 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
                             ke_acc = tk;
                         }
                     }
+                    if (fs.stage == 3) {
 #pragma unroll
-                    for (int q = 0; q < 5; ++q) *reinterpret_cast<double2 *>(fs.Uout[q] + c64) = Uo[q];
+                        for (int q = 0; q < 5; ++q) *reinterpret_cast<double2 *>(fs.Uout[q] + c64) = Uo[q];
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) *reinterpret_cast<float2 *>(fs.D[q] + cid) = Dn[q];
+                    }
                     if (per && cu < NG + 5) {  // re-read by the line's wrapped end: write after the line
                         has_def = true;
                         const int dp = (cu - NG) * NP + pr;
