@@ -9,12 +9,13 @@
 //     instructions (add / mul / fma on f32x2: one instruction for both lines),
 //   * every shared-memory access moves a 64-bit word (both lines at once), and
 //   * along y and z the two lines are x-neighbours, so the global loads,
-//     stores and cp.async copies are 8 bytes (16 for the FP64 state).
+//     stores and cp.async copies are 8 bytes (16 for the FP64 state; along z
+//     the staging copies take four lines, 16 bytes, past L1).
 // HLLC runs paired too (hllc_flux2); the other Riemann solvers and the rare
-// WENO branch of the hybrid scheme run per line on the unpacked halves.  The arithmetic of each half is the scalar
-// kernel's; only the placement of fused multiply-adds differs, so results
-// agree with it to FP32 rounding (the mixed path has an accuracy bound, not
-// a bitwise contract).
+// WENO branch of the hybrid scheme run per line on the unpacked halves.  The
+// arithmetic of each half is the scalar kernel's; only the placement of fused
+// multiply-adds differs, so results agree with it to FP32 rounding (the mixed
+// path has an accuracy bound, not a bitwise contract).
 //
 // Requires an even number of lines across the block's bundle (ny along x,
 // nx along y and z), so a pair never straddles the end of the domain and the
