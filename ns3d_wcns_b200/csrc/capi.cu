@@ -484,7 +484,7 @@ int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double d
     } else {
         StageArgsMixed a;
         for (int q = 0; q < 5; ++q) {
-            a.U0[q] = h->S[src0][q]; a.Uc[q] = h->S[srcc][q]; a.Rhs[q] = h->rhs32[q];
+            a.U0[q] = h->S[src0][q]; a.Uc[q] = h->S[srcc][q]; a.Rhs[q] = h->rhs32[q]; a.D[q] = nullptr;
             a.Uout[q] = h->S[dst][q]; a.Wout[q] = h->w32[q];
         }
         a.L = h->L64; a.L32 = h->L32; a.b = h->bc; a.dt = dt; a.gamma = h->ph.gamma; a.stage = stage;
