@@ -72,6 +72,12 @@ typedef struct ns3d_params {
     int precision;                  /* NS3D_FP64 (reference parity) | NS3D_MIXED */
     int device;                     /* CUDA device ordinal */
     int check_state;                /* 1: rk3 calls verify the state is finite */
+    int keep_rhs;                   /* 1: an RK3 step also leaves its last stage's complete
+                                       right-hand side in the RHS buffer, as runge_kutta_3
+                                       leaves it in F.rhs_* (one more write per cell in the
+                                       last stage); 0 (default): the last stage updates the
+                                       state without storing its RHS, and NS3D_RHS can be
+                                       downloaded only after ns3d_compute_rhs */
 } ns3d_params;
 
 /* GridDesc (field_structures.h:33-38). */
@@ -107,6 +113,19 @@ int ns3d_upload_primitives(ns3d_handle *h, const double *const fields[5]);
  * ghost fill.  Replaces: an initialiser + apply_boundary + primitiveToConserved
  * (main.cpp:85-99). */
 int ns3d_set_interior_primitives(ns3d_handle *h, const double *const fields[5]);
+
+/* Built-in initial states on the device, followed by the ghost fill: the
+ * state main.cpp:85-99 sets up with one of the reference's initialisers,
+ * apply_boundary and primitiveToConserved.  Replaces:
+ *   NS3D_INIT_RIEMANN_2D  initialize_riemann_2d     (initialization.cpp:516-566;
+ *                         main.cpp's default; every cell, ghosts included)
+ *   NS3D_INIT_SOD         initialize_sod_shock_tube (initialization.cpp:568-596)
+ *   NS3D_INIT_UNIFORM     initialize_uniform_field  (initialization.cpp:598-617)
+ *   NS3D_INIT_SINE_X      initialize_sine_x_field   (initialization.cpp:619-638)
+ * Cells an initialiser does not write keep their current values (the
+ * Field3D::allocate defaults on a new handle). */
+enum { NS3D_INIT_RIEMANN_2D = 0, NS3D_INIT_SOD = 1, NS3D_INIT_UNIFORM = 2, NS3D_INIT_SINE_X = 3 };
+int ns3d_initialize(ns3d_handle *h, int kind);
 
 /* Download one group (NS3D_PRIMITIVE/CONSERVED/RHS: 5 arrays; TEMPERATURE: 1)
  * in Field3D layout. */
@@ -151,6 +170,17 @@ int ns3d_total_energy(ns3d_handle *h, double *ke_out);
  *          2 nu sum_k k^2 E(k) of ana_isotropic.cpp:271-305,
  * out[5] = u_rms = sqrt(<u^2+v^2+w^2>/3) (ana_isotropic.cpp:280). */
 int ns3d_diagnostics(ns3d_handle *h, double out[6]);
+
+/* Residual norms of the last step.  Replaces: compute_diagnostics
+ * (postprocess.cpp:7-98, ns3d_func.h) with Field3D::updateResiduals
+ * (field_structures.h:500-508): out[q] = sqrt(sum over the interior of
+ * (U_q - U0_q)^2 dx^3) / max over the interior of |U_q| for q = rho, rhou,
+ * rhov, rhow, E (F.global_res_rho ... F.global_res_E), U the state after the
+ * step and U0 the state the step started from.  Valid right after
+ * ns3d_rk3_step / ns3d_rk3_steps / ns3d_time_advance; a download, upload,
+ * ghost fill or adjoint call in between reuses the step-start buffer, and the
+ * call then returns NS3D_ERR_STATE. */
+int ns3d_residuals(ns3d_handle *h, double out[5]);
 
 /* The dt schedule of time_advance (maincycle.cpp:18-56) without I/O:
  * advances from *time until t_end or max_steps, adaptive dt when
@@ -252,6 +282,13 @@ int ns3d_debug_visc_vjp(double mu0, double S, double cp_over_pr, const double *x
  * InviscousFlux.cpp:270-846); for unit tests of the flux functions. */
 int ns3d_debug_riemann(int direction, int riemann, double gamma, const double UL[5], const double UR[5],
                        double F[5]);
+/* The MDCD_HYBRID discontinuity detector of the FP64 sweeps evaluated on the
+ * device: smooth_out[i] = 1 when sai(a, b) > 0.4 at the centre of the
+ * five-point stencil stencils[5i .. 5i+4] (the reference's sigma test of one
+ * centre, mdcd_hybrid_interpolate, interpolation.cpp:149-160), else 0.
+ * n <= 2^26.  For tests of near-threshold decisions; allocates and frees its
+ * own device buffers. */
+int ns3d_debug_mdcd_detector(int device, long n, const double *stencils, int *smooth_out);
 /* Runs the bounded mbarrier wait of the TMA kernels against a barrier that
  * never completes (armed for bytes no copy delivers): each block gives up
  * after `polls` polls, writes the device error word (returned in *code_out)
@@ -259,6 +296,35 @@ int ns3d_debug_riemann(int direction, int riemann, double gamma, const double UL
  * entry points do when one of their TMA waits runs out.  No counterpart in
  * the reference; for tests of the failure path. */
 int ns3d_debug_wait_timeout(int device, unsigned polls, int *code_out);
+
+/* ------------------------------------------------ z-slab decomposition
+ * A handle holding one rank's z-slab of a domain split along z over several
+ * GPUs.  Replaces the reference's per-rank decomposition (build_cart_decomp /
+ * compute_local_desc, field_structures.h:1062-1115) and its three exchanges
+ * per stage (exchange_halos_physical :936-994, exchange_halos_halfnode_flux
+ * :998-1056, exchange_halos_viscous_flux :877-932) by one: the local grid
+ * holds the rank's owned interior planes [z_begin, z_end) plus six halo
+ * planes on every side that borders another rank, whose primitives and
+ * temperature the caller refreshes after every stage; the face and node
+ * viscous fluxes the owned cells need are then computed locally from the
+ * same inputs, so the owned cells equal a single-domain run bit for bit.
+ * ns3d_set_slab: the owned planes (local interior indices; six planes or
+ * more, and six halo planes on each bordering side; the local z boundary
+ * types must be non-periodic -- their treatment stays inside the halo) and,
+ * when dz > 0, the global grid spacing (so the local dz is the global one bit
+ * for bit).  The x/y sweeps then run over the owned planes, the viscous
+ * fluxes over the owned planes and three halo planes each side, the z-sweep
+ * updates owned cells only, and every reduction (time step, kinetic energy,
+ * diagnostics) counts owned cells only.  ns3d_rk3_step / _steps /
+ * time_advance and the adjoint return NS3D_ERR_STATE / NS3D_ERR_CONFIG on a
+ * slab.
+ * ns3d_rk3_stage: one RK3 stage (1, 2, 3, in order) of a step, enqueued on
+ * the handle's stream without synchronising; the halo planes of the stage's
+ * result are then exchanged through the pointers of ns3d_device_fields
+ * (NS3D_PRIMITIVE and NS3D_TEMPERATURE), as runge_kutta_3's apply_boundary
+ * does after every stage (range_kutta.cpp:61-63). */
+int ns3d_set_slab(ns3d_handle *h, int z_begin, int z_end, double dz);
+int ns3d_rk3_stage(ns3d_handle *h, int stage, double dt);
 
 /* ---------------------------------------- scratch-free CFL time step
  * No counterpart in the reference.  For host codes that cannot let a library
@@ -277,9 +343,11 @@ int ns3d_debug_wait_timeout(int device, unsigned polls, int *code_out);
  * per-block partials (NS3D_NOALLOC_MAX_BLOCKS doubles) that every GPU which
  * loads the library holds until the process exits.  All calls share that
  * array, so calls that overlap on a GPU (other streams or host threads) race
- * on it: serialise them.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture. */
+ * on it: serialise them.  The first call in a CUDA context looks up the
+ * array's device address (cudaGetSymbolAddress) and caches it for that
+ * context; make that first call before any stream capture, once per device,
+ * and again after cudaDeviceReset or a switch to another context on the
+ * device (each of which loads the library's module at a new address). */
 #define NS3D_NOALLOC_MAX_BLOCKS 16384
 #define NS3D_NOALLOC_MAX_CELLS (16384L * 256 * 32)
 int ns3d_compute_timestep_noalloc(const double *const d_fields[5], int nx, int ny, int nz, double gamma,

@@ -22,12 +22,13 @@ STATUS = {0: "NS3D_OK", -1: "NS3D_ERR_INVALID_ARG", -2: "NS3D_ERR_CONFIG", -3: "
 # every entry point declared in include/ns3d_b200.h
 EXPORTS = [
     "ns3d_params_default", "ns3d_status_string", "ns3d_create", "ns3d_destroy", "ns3d_last_error",
-    "ns3d_field_dims", "ns3d_upload_primitives", "ns3d_set_interior_primitives", "ns3d_download",
+    "ns3d_field_dims", "ns3d_upload_primitives", "ns3d_initialize", "ns3d_set_interior_primitives", "ns3d_download",
     "ns3d_apply_boundary", "ns3d_compute_rhs", "ns3d_rk3_step", "ns3d_rk3_steps",
-    "ns3d_compute_timestep", "ns3d_total_energy", "ns3d_diagnostics", "ns3d_time_advance",
+    "ns3d_compute_timestep", "ns3d_total_energy", "ns3d_diagnostics", "ns3d_residuals", "ns3d_time_advance",
     "ns3d_device_fields", "ns3d_set_stream", "ns3d_synchronize", "ns3d_last_launch_count",
-    "ns3d_profile", "ns3d_profile_report", "ns3d_compute_timestep_noalloc",
-    "ns3d_debug_face_vjp", "ns3d_debug_visc_vjp", "ns3d_debug_riemann", "ns3d_debug_wait_timeout", "ns3d_vjp_rhs", "ns3d_vjp_rk3_step",
+    "ns3d_profile", "ns3d_profile_report", "ns3d_compute_timestep_noalloc", "ns3d_set_slab", "ns3d_rk3_stage",
+    "ns3d_debug_face_vjp", "ns3d_debug_visc_vjp", "ns3d_debug_riemann", "ns3d_debug_wait_timeout",
+    "ns3d_debug_mdcd_detector", "ns3d_vjp_rhs", "ns3d_vjp_rk3_step",
     "ns3d_adjoint_kinetic_energy", "ns3d_batch_create", "ns3d_batch_destroy", "ns3d_batch_last_error",
     "ns3d_batch_set_interior_primitives", "ns3d_batch_run", "ns3d_batch_autotune", "ns3d_batch_set_config",
     "ns3d_batch_query", "ns3d_batch_download",
@@ -39,7 +40,8 @@ class Params(C.Structure):
                 ("cfl", C.c_double), ("dt_fixed", C.c_double), ("mdcd_diss", C.c_double),
                 ("mdcd_disp", C.c_double), ("sutherland_s", C.c_double), ("interpolation", C.c_int),
                 ("riemann_solver", C.c_int), ("char_recon", C.c_int), ("bc", C.c_int * 6),
-                ("precision", C.c_int), ("device", C.c_int), ("check_state", C.c_int)]
+                ("precision", C.c_int), ("device", C.c_int), ("check_state", C.c_int),
+                ("keep_rhs", C.c_int)]
 
 
 class Grid(C.Structure):
@@ -76,6 +78,7 @@ def load() -> C.CDLL:
     lib.ns3d_field_dims.argtypes = [h, C.POINTER(C.c_int)]
     lib.ns3d_upload_primitives.argtypes = [h, C.POINTER(dp)]
     lib.ns3d_set_interior_primitives.argtypes = [h, C.POINTER(dp)]
+    lib.ns3d_initialize.argtypes = [h, C.c_int]
     lib.ns3d_download.argtypes = [h, C.c_int, C.POINTER(dp)]
     lib.ns3d_apply_boundary.argtypes = [h]
     lib.ns3d_compute_rhs.argtypes = [h]
@@ -84,9 +87,12 @@ def load() -> C.CDLL:
     lib.ns3d_compute_timestep.argtypes = [h, dp]
     lib.ns3d_total_energy.argtypes = [h, dp]
     lib.ns3d_diagnostics.argtypes = [h, dp]
+    lib.ns3d_residuals.argtypes = [h, dp]
     lib.ns3d_time_advance.argtypes = [h, C.c_double, C.c_int, dp, C.POINTER(C.c_int)]
     lib.ns3d_device_fields.argtypes = [h, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_long)]
     lib.ns3d_set_stream.argtypes = [h, C.c_void_p]
+    lib.ns3d_set_slab.argtypes = [h, C.c_int, C.c_int, C.c_double]
+    lib.ns3d_rk3_stage.argtypes = [h, C.c_int, C.c_double]
     lib.ns3d_synchronize.argtypes = [h]
     lib.ns3d_last_launch_count.argtypes = [h, C.POINTER(C.c_long)]
     lib.ns3d_profile.argtypes = [h, C.c_int]
@@ -108,6 +114,7 @@ def load() -> C.CDLL:
     lib.ns3d_debug_visc_vjp.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp, dp, dp, dp, dp]
     lib.ns3d_debug_riemann.argtypes = [C.c_int, C.c_int, C.c_double, dp, dp, dp]
     lib.ns3d_debug_wait_timeout.argtypes = [C.c_int, C.c_uint, C.POINTER(C.c_int)]
+    lib.ns3d_debug_mdcd_detector.argtypes = [C.c_int, C.c_long, dp, C.POINTER(C.c_int)]
     lib.ns3d_compute_timestep_noalloc.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_double,
                                                   C.c_double, C.c_double, C.c_void_p, C.c_void_p]
     _lib = lib

@@ -301,8 +301,9 @@ def format_solver_in(P: SolverParams, G: GridDesc, extra: bool = False) -> str:
     names = ["bc_xmin", "bc_xmax", "bc_ymin", "bc_ymax", "bc_zmin", "bc_zmax"]
     for n, b in zip(names, P.bcs):
         lines.append(f"{n} = {BCType(b).name}")
-    lines += ["Post_BasicField = False", "IsotropicAnalyse = False", "monitor_Res = False",
-              "monitor_Energy = False"]
+    tf = lambda b: "True" if b else "False"
+    lines += [f"Post_BasicField = {tf(P.post_basicfield)}", f"IsotropicAnalyse = {tf(P.isotropic_analyse)}",
+              f"monitor_Res = {tf(P.monitor_res)}", f"monitor_Energy = {tf(P.monitor_energy)}"]
     if extra:
         lines.append(f"sutherland_s = {fmt(P.S_ref)}")
         lines.append(f"precision = {'fp64' if P.precision == Precision.FP64 else 'mixed'}")
@@ -322,6 +323,8 @@ def make_params(n=(32, 32, 32), L=(2 * math.pi,) * 3, gamma=1.4, Pr=0.72, Ma=0.3
     P.interpolation, P.riemann_solver, P.char_recon = Interpolation(interpolation), RiemannSolver(riemann), bool(char_recon)
     P.mdcd_disp, P.mdcd_diss = mdcd_disp, mdcd_diss
     (P.bc_xmin, P.bc_xmax, P.bc_ymin, P.bc_ymax, P.bc_zmin, P.bc_zmax) = [BCType(b) for b in bcs]
+    # output and monitoring off unless asked for
+    P.post_basicfield = P.isotropic_analyse = P.monitor_res = P.monitor_energy = False
     for k, v in kw.items():
         setattr(P, k, v)
     P2, G2, _ = parse_solver_params(format_solver_in(P, G))

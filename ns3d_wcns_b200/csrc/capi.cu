@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -25,12 +26,13 @@ using namespace ns3d;
 // Sums over interior cells: [0] KE (0.5 rho |u|^2 dV, postprocess.cpp:119-122),
 // [1] sum |grad u|^2, [2] sum mu(T), [3] sum rho, [4] sum |u|^2.
 template <typename R>
-__global__ void __launch_bounds__(RED_THREADS) diag_kernel(ViscArgs<R> a, double vol, double *partials) {
+__global__ void __launch_bounds__(RED_THREADS) diag_kernel(ViscArgs<R> a, double vol, double *partials, int zlo,
+                                                            int nzo) {
     const Layout &L = a.L;
-    const long ncell = (long)L.nx * L.ny * L.nz;
+    const long ncell = (long)L.nx * L.ny * nzo;
     double acc[5] = {0, 0, 0, 0, 0};
     for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = (int)(t / ((long)L.nx * L.ny));
+        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = zlo + (int)(t / ((long)L.nx * L.ny));
         const long c = L.at(i + NG, j + NG, k + NG);
         const double rho = a.W[0][c], u = a.W[1][c], v = a.W[2][c], w = a.W[3][c];
         const double kinetic = 0.5 * rho * (u * u + v * v + w * w);
@@ -51,11 +53,11 @@ __global__ void __launch_bounds__(RED_THREADS) diag_kernel(ViscArgs<R> a, double
 
 // Minimum CFL bound over interior cells (compute_timestep, timestep.cpp:5-23).
 __global__ void __launch_bounds__(RED_THREADS) dt_kernel64(const double *const *Wp, Layout L, double gamma,
-                                                           double dx, double *partials) {
-    const long ncell = (long)L.nx * L.ny * L.nz;
+                                                           double dx, double *partials, int zlo, int nzo) {
+    const long ncell = (long)L.nx * L.ny * nzo;
     double m = 1e9;
     for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = (int)(t / ((long)L.nx * L.ny));
+        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = zlo + (int)(t / ((long)L.nx * L.ny));
         const long c = L.at(i + NG, j + NG, k + NG);
         double U[5];
         p2c_exact(Wp[0][c], Wp[1][c], Wp[2][c], Wp[3][c], Wp[4][c], gamma, U);
@@ -65,11 +67,11 @@ __global__ void __launch_bounds__(RED_THREADS) dt_kernel64(const double *const *
 }
 
 __global__ void __launch_bounds__(RED_THREADS) dt_kernel_mixed(const double *const *Up, Layout L, double gamma,
-                                                               double dx, double *partials) {
-    const long ncell = (long)L.nx * L.ny * L.nz;
+                                                               double dx, double *partials, int zlo, int nzo) {
+    const long ncell = (long)L.nx * L.ny * nzo;
     double m = 1e9;
     for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = (int)(t / ((long)L.nx * L.ny));
+        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = zlo + (int)(t / ((long)L.nx * L.ny));
         const long c = L.at(i + NG, j + NG, k + NG);
         double U[5] = {Up[0][c], Up[1][c], Up[2][c], Up[3][c], Up[4][c]};
         m = fmin(m, cfl_bound(U, gamma, dx));
@@ -122,11 +124,12 @@ __global__ void __launch_bounds__(256) min_combine_kernel(const double *part, lo
 // Non-finite / non-positive state detector: counts interior cells with a
 // non-finite value or rho <= 0 or p <= 0.
 template <typename R>
-__global__ void __launch_bounds__(RED_THREADS) check_kernel(const R *const *Wp, Layout L, double *partials) {
-    const long ncell = (long)L.nx * L.ny * L.nz;
+__global__ void __launch_bounds__(RED_THREADS) check_kernel(const R *const *Wp, Layout L, double *partials, int zlo,
+                                                             int nzo) {
+    const long ncell = (long)L.nx * L.ny * nzo;
     double bad = 0;
     for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = (int)(t / ((long)L.nx * L.ny));
+        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = zlo + (int)(t / ((long)L.nx * L.ny));
         const long c = L.at(i + NG, j + NG, k + NG);
         bool ok = true;
 #pragma unroll
@@ -136,6 +139,52 @@ __global__ void __launch_bounds__(RED_THREADS) check_kernel(const R *const *Wp, 
     }
     double v[1] = {bad};
     block_sum<1>(v, partials + blockIdx.x);
+}
+
+// Residual norms of a step (compute_diagnostics, postprocess.cpp:7-98, with
+// Field3D::updateResiduals, field_structures.h:500-508): per conserved
+// variable, the sum over interior cells of (U - U0)^2 dx^3 and the largest
+// |U|, U the state after the step and U0 the state it started from (plain
+// path: both the exact p2c of the stored primitives, so the same bits as the
+// reference's arrays; mixed path: the stored FP64 conserved states).
+template <bool MIXED>
+__global__ void __launch_bounds__(RED_THREADS) residual_kernel(const double *const *Sn, const double *const *S0,
+                                                               Layout L, double gamma, double dx3,
+                                                               double *partials, int zlo, int nzo) {
+    const long ncell = (long)L.nx * L.ny * nzo;
+    double sq[5] = {0, 0, 0, 0, 0}, mx[5] = {0, 0, 0, 0, 0};
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % L.nx), j = (int)((t / L.nx) % L.ny), k = zlo + (int)(t / ((long)L.nx * L.ny));
+        const long c = L.at(i + NG, j + NG, k + NG);
+        double U[5], U0[5];
+        if constexpr (MIXED) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { U[q] = Sn[q][c]; U0[q] = S0[q][c]; }
+        } else {
+            p2c_exact(Sn[0][c], Sn[1][c], Sn[2][c], Sn[3][c], Sn[4][c], gamma, U);
+            p2c_exact(S0[0][c], S0[1][c], S0[2][c], S0[3][c], S0[4][c], gamma, U0);
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const double r = U[q] - U0[q];
+            sq[q] += r * r * dx3;
+            mx[q] = fmax(mx[q], fabs(U[q]));
+        }
+    }
+    block_sum_max<5>(sq, mx, partials + 10 * blockIdx.x);
+}
+
+// Fixed-order combination of the residual partials: sums of values 0-4,
+// maxima of values 5-9.
+__global__ void residual_combine_kernel(const double *partials, int nblocks, double *out) {
+    if (threadIdx.x >= 10) return;
+    const int q = threadIdx.x;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        const double x = partials[(long)b * 10 + q];
+        s = q < 5 ? s + x : fmax(s, x);
+    }
+    out[q] = s;
 }
 
 // Fixed-order combination of per-block partials (nv values per block).
@@ -263,6 +312,14 @@ struct ns3d_handle {
     long cfl_nblocks = 0;         // capacity of cfl_part / ke_part
     long cfl_count = 0;           // partials the last stage-3 launch wrote
     bool cfl_valid = false;       // cfl_part describes the current state
+    bool rhs_complete = false;    // the RHS buffer holds a complete right-hand side
+    bool prev_valid = false;      // buffer (s0 + 2) % 3 holds the state the last step started from
+    int zlo = 0, zhi = 0;         // owned interior z-planes (a z-slab's halo planes lie outside)
+    bool visc_valid = false;      // the node viscous fluxes describe the current state
+    bool diag_separate = false;   // ns3d_diagnostics by its separate gradient pass (NS3D_DIAG_SEPARATE=1)
+    double *visc_red = nullptr;   // per-block diagnostics sums of the viscous kernel (5 per block)
+    long visc_nblocks = 0;
+    int step_start = -1;          // ns3d_rk3_stage: buffer the current step started from
     double *scalars = nullptr;
     int red_blocks = 0;
     bool has_state = false;
@@ -364,6 +421,7 @@ SweepArgs<R> sweep_args(ns3d_handle *h, int dir) {
     static const int comp[3][4] = {{0, 3, 4, 6}, {3, 1, 5, 7}, {4, 5, 2, 8}};
     for (int q = 0; q < 4; ++q) a.V[q] = (const R *)h->visc[comp[dir][q]];
     a.done = h->dev_loop ? &h->clock->done : nullptr;
+    a.zlo = h->zlo; a.zhi = h->zhi;
     a.fs = FusedStage{};  // stage 0: the sweep writes the right-hand side
     return a;
 }
@@ -421,27 +479,46 @@ ViscArgs<R> visc_args(ns3d_handle *h) {
     a.err = h->dev_err;
     a.done = h->dev_loop ? &h->clock->done : nullptr;
     a.cp_over_pr = (R)(h->ph.Cp / h->ph.Pr);
+    // the owned planes and the three either side whose fluxes the z-divergence reads
+    a.zlo = h->zlo > 0 ? h->zlo - 3 : 0;
+    a.zhi = h->zhi < a.L.nz ? h->zhi + 3 : a.L.nz;
+    a.red = nullptr;
+    a.rlo = h->zlo; a.rhi = h->zhi;
+    a.vol = h->ph.dx * h->ph.dy * h->ph.dz;
     return a;
+}
+
+template <typename R>
+int visc_launch(ns3d_handle *h, double *red, long *nblocks = nullptr) {
+    ViscArgs<R> va = visc_args<R>(h);
+    va.red = red;
+    dim3 g((va.L.nx + VTX - 1) / VTX, (va.L.ny + VTY - 1) / VTY, (va.zhi - va.zlo + VZC - 1) / VZC);
+    if (nblocks) *nblocks = (long)g.x * g.y * g.z;
+    ViscMaps maps;
+    for (int q = 0; q < 3; ++q) maps.m[q] = sizeof(R) == 8 ? h->tmW64[h->s0][q] : h->tmW32[q];
+    maps.m[3] = sizeof(R) == 8 ? h->tmT64 : h->tmT32;
+    prof_begin(h, "viscous_flux");
+    if (va.periodic[0] && va.periodic[1] && va.periodic[2])
+        viscous_flux_kernel<R, true><<<g, dim3(VTX, VTY), 0, h->stream>>>(va, maps);
+    else
+        viscous_flux_kernel<R, false><<<g, dim3(VTX, VTY), 0, h->stream>>>(va, maps);
+    prof_end(h);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "viscous kernel");
+    return NS3D_OK;
 }
 
 template <typename R>
 int rhs_impl(ns3d_handle *h, const FusedStage *fs = nullptr) {
     cudaStream_t st = h->stream;
     cudaError_t e;
-    if (h->ph.mu != 0.0) {  // Re = inf: the viscous terms are exactly zero
-        ViscArgs<R> va = visc_args<R>(h);
-        dim3 g((va.L.nx + VTX - 1) / VTX, (va.L.ny + VTY - 1) / VTY, (va.L.nz + VZC - 1) / VZC);
-        ViscMaps maps;
-        for (int q = 0; q < 3; ++q) maps.m[q] = sizeof(R) == 8 ? h->tmW64[h->s0][q] : h->tmW32[q];
-        maps.m[3] = sizeof(R) == 8 ? h->tmT64 : h->tmT32;
-        prof_begin(h, "viscous_flux");
-        if (va.periodic[0] && va.periodic[1] && va.periodic[2])
-            viscous_flux_kernel<R, true><<<g, dim3(VTX, VTY), 0, st>>>(va, maps);
-        else
-            viscous_flux_kernel<R, false><<<g, dim3(VTX, VTY), 0, st>>>(va, maps);
-        prof_end(h);
-        h->launches += 1;
-        CK(h, cudaGetLastError(), "viscous kernel");
+    // the node fluxes of this state may be there already (ns3d_diagnostics
+    // computes them with its sums); never inside a captured time loop
+    const bool have_visc = h->visc_valid && !h->dev_loop;
+    h->visc_valid = false;
+    if (h->ph.mu != 0.0 && !have_visc) {  // Re = inf: the viscous terms are exactly zero
+        const int r = visc_launch<R>(h, nullptr);
+        if (r) return r;
     }
     prof_begin(h, "sweep_x");
     e = sweep_x(sweep_args<R>(h, 0), st); if (e != cudaSuccess) return cuda_fail(h, e, "sweep_x");
@@ -459,12 +536,16 @@ int rhs_impl(ns3d_handle *h, const FusedStage *fs = nullptr) {
 }
 
 int compute_rhs_async(ns3d_handle *h) {
-    return h->mixed ? rhs_impl<float>(h) : rhs_impl<double>(h);
+    const int r = h->mixed ? rhs_impl<float>(h) : rhs_impl<double>(h);
+    h->rhs_complete = r == NS3D_OK;
+    h->visc_valid = r == NS3D_OK && h->ph.mu != 0.0 && !h->dev_loop;  // node fluxes of the current state
+    return r;
 }
 
 // stage: 1..3 RK stages, 0 = ghost fill of the current state.
 int stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, double dt) {
     cudaStream_t st = h->stream;
+    h->visc_valid = false;
     dim3 g = cell_grid(h->L64, true, STAGE_THREADS);
     double *cfl = stage == 3 ? h->cfl_part : nullptr;  // the next step's CFL bound
     if (!h->mixed) {
@@ -532,9 +613,12 @@ int rk_stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, doubl
         f.vol = h->ph.dx * h->ph.dy * h->ph.dz;
         f.cfl_part = stage == 3 ? h->cfl_part : nullptr;
         f.ke_part = stage == 3 ? h->ke_part : nullptr;
+        f.keep_rhs = stage == 3 && h->P.keep_rhs;
         h->cfl_valid = false;
+        h->rhs_complete = false;
         int r = rhs_impl<float>(h, &f);
         if (r) return r;
+        h->rhs_complete = f.keep_rhs != 0;
         StageArgsMixed a;
         for (int q = 0; q < 5; ++q) {
             a.U0[q] = h->S[src0][q]; a.Uc[q] = nullptr; a.Rhs[q] = h->rhs32[q];
@@ -569,9 +653,12 @@ int rk_stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, doubl
     f.vol = h->ph.dx * h->ph.dy * h->ph.dz;
     f.cfl_part = stage == 3 ? h->cfl_part : nullptr;
     f.ke_part = stage == 3 ? h->ke_part : nullptr;
+    f.keep_rhs = stage == 3 && h->P.keep_rhs;
     h->cfl_valid = false;
+    h->rhs_complete = false;
     int r = rhs_impl<double>(h, &f);
     if (r) return r;
+    h->rhs_complete = f.keep_rhs != 0;
     StageArgs64 a;
     for (int q = 0; q < 5; ++q) {
         a.W0[q] = h->S[src0][q]; a.Wc[q] = h->S[srcc][q]; a.Rhs[q] = h->rhs64[q]; a.Wout[q] = h->S[dst][q];
@@ -614,8 +701,10 @@ int rk3_async(ns3d_handle *h, double dt) {
     return NS3D_OK;
 }
 
-int reduce_combine(ns3d_handle *h, int nv, int mode, double *host_out) {
-    combine_kernel<<<1, 32, 0, h->stream>>>(h->partials, h->red_blocks, nv, mode, h->scalars);
+int reduce_combine(ns3d_handle *h, int nv, int mode, double *host_out, const double *part = nullptr,
+                   long nblocks = 0) {
+    combine_kernel<<<1, 32, 0, h->stream>>>(part ? part : h->partials, part ? (int)nblocks : h->red_blocks, nv, mode,
+                                            h->scalars);
     h->launches += 1;
     CK(h, cudaGetLastError(), "combine");
     CK(h, cudaMemcpyAsync(host_out, h->scalars, sizeof(double) * nv, cudaMemcpyDeviceToHost, h->stream), "copy scalars");
@@ -625,10 +714,10 @@ int reduce_combine(ns3d_handle *h, int nv, int mode, double *host_out) {
 
 int check_state(ns3d_handle *h) {
     if (!h->mixed)
-        check_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->partials);
+        check_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->partials, h->zlo, h->zhi - h->zlo);
     else
         check_kernel<float><<<h->red_blocks, RED_THREADS, 0, h->stream>>>((const float *const *)(h->dptr + 25), h->L32,
-                                                                           h->partials);
+                                                                           h->partials, h->zlo, h->zhi - h->zlo);
     h->launches += 1;
     CK(h, cudaGetLastError(), "check kernel");
     double bad = 0;
@@ -657,8 +746,11 @@ __global__ void from_interior_kernel(const double *src, double *dst, Layout L) {
     dst[((long)k * L.sy + j) * L.sx + i] = in ? src[((long)(k - NG) * L.ny + (j - NG)) * L.nx + (i - NG)] : 0.0;
 }
 
+bool is_slab(const ns3d_handle *h) { return h->zlo != 0 || h->zhi != h->G.nz; }
+
 bool adjoint_supported(const ns3d_handle *h, std::string &why) {
     if (h->mixed) { why = "adjoint: plain FP64 path only"; return false; }
+    if (is_slab(h)) { why = "adjoint: whole domains only (not a z-slab)"; return false; }
     if (!(h->bc.periodic[0] && h->bc.periodic[1] && h->bc.periodic[2])) {
         why = "adjoint: periodic boundaries in all directions only"; return false;
     }
@@ -773,6 +865,7 @@ int rk3_async_store(ns3d_handle *h, double dt, double *const st[3][5]) {
 
 // T of the current state (after the state buffer was overwritten by a copy)
 int refresh_T(ns3d_handle *h) {
+    h->visc_valid = false;
     dim3 g = cell_grid(h->L64, true, 128);
     temp_kernel64<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), h->T64, h->L64, h->ph.Rgas);
     h->launches += 1;
@@ -883,6 +976,8 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     if (cudaSetDevice(h->device) != cudaSuccess) { delete h; return NS3D_ERR_NO_DEVICE; }
     h->L64 = make_layout<double>(grid->nx, grid->ny, grid->nz);
     h->L32 = make_layout<float>(grid->nx, grid->ny, grid->nz);
+    h->zlo = 0;
+    h->zhi = grid->nz;
     if (ghost_count(h->L64) >= (1L << 31)) { delete h; return NS3D_ERR_SIZE; }  // 32-bit ghost decode
     // the mixed path's FP32 stage increments live inside an FP64 state plane
     if ((size_t)h->L32.plane * 4 > (size_t)h->L64.plane * 8) { delete h; return NS3D_ERR_CONFIG; }
@@ -926,7 +1021,7 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     bytes += h->mixed ? 11 * p32 : 6 * p64;                    // (w32 + rhs32 + T32) or (rhs64 + T64)
     bytes += 9 * vis_elems * (h->mixed ? 4 : 8);               // viscous node fluxes
     bytes += 256 * 32;                                         // pointer tables
-    bytes += ((size_t)h->red_blocks * 8 * 8 + 255) / 256 * 256;  // partials
+    bytes += ((size_t)h->red_blocks * 10 * 8 + 255) / 256 * 256;  // partials
     bytes += 256;                                              // scalars
     {
         const dim3 sg = cell_grid(h->L64, true, STAGE_THREADS);
@@ -934,6 +1029,11 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     }
     bytes += 2 * (((size_t)h->cfl_nblocks * 8 + 255) / 256 * 256);  // stage CFL minima, kinetic energy
     bytes += 256;                                              // device clock
+    {
+        const long vb = (long)((grid->nx + VTX - 1) / VTX) * ((grid->ny + VTY - 1) / VTY) * ((grid->nz + VZC - 1) / VZC);
+        h->visc_nblocks = vb;
+        bytes += ((size_t)vb * 5 * 8 + 255) / 256 * 256;      // viscous-kernel diagnostics sums
+    }
     cudaError_t e = cudaMalloc(&h->pool, bytes);
     if (e != cudaSuccess) { delete h; cudaGetLastError(); return NS3D_ERR_OOM; }
     h->pool_bytes = bytes;
@@ -950,7 +1050,7 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     }
     for (int q = 0; q < 9; ++q) { h->visc[q] = p; p += vis_elems * (h->mixed ? 4 : 8); }
     h->dptr = (double **)p; p += 256 * 32;
-    h->partials = (double *)p; p += ((size_t)h->red_blocks * 8 * 8 + 255) / 256 * 256;
+    h->partials = (double *)p; p += ((size_t)h->red_blocks * 10 * 8 + 255) / 256 * 256;
     h->scalars = (double *)p;
     h->dev_err = (int *)((char *)p + 128);
     p += 256;
@@ -959,6 +1059,12 @@ int ns3d_create(const ns3d_params *params, const ns3d_grid *grid, ns3d_handle **
     h->ke_part = (double *)p;
     p += ((size_t)h->cfl_nblocks * 8 + 255) / 256 * 256;
     h->clock = (DevClock *)p;
+    p += 256;
+    h->visc_red = (double *)p;
+    {
+        const char *ds = std::getenv("NS3D_DIAG_SEPARATE");  // the separate gradient pass, for comparison
+        h->diag_separate = ds && ds[0] == '1';
+    }
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { cudaFree(h->pool); delete h; return NS3D_ERR_CUDA; }
     h->own_stream = true;
@@ -1099,9 +1205,49 @@ __global__ void upload_mixed_kernel(const double *const *Wp, double *const *Up, 
     T32[c32] = (float)(W[4] / (W[0] * Rgas));
 }
 
+// The reference's built-in initialisers (initialization.cpp:516-638) on the
+// device, writing primitives into a padded FP64 state buffer: the same
+// cells, formulas and operation order (x = (ox + i - ngx + 0.5) dx with
+// ox = 0 on one rank).  riemann_2d fills every cell including the ghosts;
+// the others fill the interior only.
+__global__ void init_kernel(double *const *Wp, Layout L, int kind, double dx, double dy, double Lx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= L.sx) return;
+    const bool interior = i >= NG && i < NG + L.nx && j >= NG && j < NG + L.ny && k >= NG && k < NG + L.nz;
+    double rho, u, v, w, p;
+    const double x = ((double)(i - NG) + 0.5) * dx;
+    if (kind == NS3D_INIT_RIEMANN_2D) {
+        // initialize_riemann_2d, initialization.cpp:516-566 (four quadrants about (0.5, 0.5))
+        const double y = ((double)(j - NG) + 0.5) * dy;
+        w = 0.0;
+        if (x >= 0.5 && y >= 0.5) { rho = 1.1; u = 0.0; v = 0.0; p = 1.1; }
+        else if (x < 0.5 && y >= 0.5) { rho = 0.5065; u = 0.8939; v = 0.0; p = 0.35; }
+        else if (x < 0.5 && y < 0.5) { rho = 1.1; u = 0.8939; v = 0.8939; p = 1.1; }
+        else { rho = 0.5065; u = 0.0; v = 0.8939; p = 0.35; }
+    } else {
+        if (!interior) return;
+        if (kind == NS3D_INIT_SOD) {
+            // initialize_sod_shock_tube, initialization.cpp:568-596 (x_mid = 0.5 nx dx)
+            const double x_mid = 0.5 * L.nx * dx;
+            v = 0.0; w = 0.0; u = 0.0;
+            if (x < x_mid) { rho = 1.0; p = 1.0; } else { rho = 0.125; p = 0.1; }
+        } else if (kind == NS3D_INIT_UNIFORM) {
+            // initialize_uniform_field, initialization.cpp:598-617
+            rho = 1.0; u = 1.0; v = 1.0; w = 1.0; p = 1.0;
+        } else {
+            // initialize_sine_x_field, initialization.cpp:619-638: u = sin(2 pi x / Lx)
+            rho = 1.0; v = 0.0; w = 0.0; p = 1.0;
+            u = sin(2.0 * M_PI * x / Lx);
+        }
+    }
+    const long c = L.at(i, j, k);
+    Wp[0][c] = rho; Wp[1][c] = u; Wp[2][c] = v; Wp[3][c] = w; Wp[4][c] = p;
+}
+
 static int finish_upload(ns3d_handle *h, int b, bool apply_bc) {
     const int dst = (b + 1) % 3, dst2 = (b + 2) % 3;
     int r;
+    h->visc_valid = false;
     if (!h->mixed) {
         if (!apply_bc) {
             dim3 g = cell_grid(h->L64, true, 128);
@@ -1130,6 +1276,7 @@ static int finish_upload(ns3d_handle *h, int b, bool apply_bc) {
 
 int ns3d_upload_primitives(ns3d_handle *h, const double *const fields[5]) {
     if (!h || !fields) return NS3D_ERR_INVALID_ARG;
+    h->prev_valid = false;  // the free state buffers are scratch here
     for (int q = 0; q < 5; ++q) if (!fields[q]) return NS3D_ERR_INVALID_ARG;
     int r = set_device(h); if (r) return r;
     h->launches = 0;
@@ -1145,6 +1292,7 @@ int ns3d_upload_primitives(ns3d_handle *h, const double *const fields[5]) {
 
 int ns3d_set_interior_primitives(ns3d_handle *h, const double *const fields[5]) {
     if (!h || !fields) return NS3D_ERR_INVALID_ARG;
+    h->prev_valid = false;  // the free state buffers are scratch here
     for (int q = 0; q < 5; ++q) if (!fields[q]) return NS3D_ERR_INVALID_ARG;
     int r = set_device(h); if (r) return r;
     h->launches = 0;
@@ -1178,8 +1326,39 @@ int ns3d_set_interior_primitives(ns3d_handle *h, const double *const fields[5]) 
     return NS3D_OK;
 }
 
+int ns3d_initialize(ns3d_handle *h, int kind) {
+    if (!h || kind < NS3D_INIT_RIEMANN_2D || kind > NS3D_INIT_SINE_X) return NS3D_ERR_INVALID_ARG;
+    h->prev_valid = false;  // the free state buffers are scratch here
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    const Layout &L = h->L64;
+    const int b = (h->s0 + 1) % 3;
+    // the cells the initialiser does not write keep their current values
+    // (initially the Field3D::allocate defaults), as in the reference
+    if (h->mixed) {
+        dim3 g = cell_grid(L, true, 128);
+        derive_kernel_mixed<<<g, 128, 0, h->stream>>>(state_table(h, h->s0), state_table(h, b), L, h->ph.gamma,
+                                                       h->ph.Rgas, NS3D_PRIMITIVE);
+        h->launches += 1;
+    } else {
+        for (int q = 0; q < 5; ++q)
+            CK(h, cudaMemcpyAsync(h->S[b][q], h->S[h->s0][q], L.plane * 8, cudaMemcpyDeviceToDevice, h->stream), "copy");
+    }
+    init_kernel<<<cell_grid(L, true, 128), 128, 0, h->stream>>>(state_table(h, b), L, kind, h->ph.dx, h->ph.dy,
+                                                                 h->G.Lx);
+    h->launches += 1;
+    CK(h, cudaGetLastError(), "initialiser");
+    // apply_boundary + primitiveToConserved (main.cpp:98-99)
+    if ((r = finish_upload(h, b, true))) return r;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    h->has_state = true;
+    h->cfl_valid = false;
+    return NS3D_OK;
+}
+
 int ns3d_download(ns3d_handle *h, int what, double *const out[]) {
     if (!h || !out) return NS3D_ERR_INVALID_ARG;
+    h->prev_valid = false;  // the free state buffers are scratch here
     if (what < NS3D_PRIMITIVE || what > NS3D_TEMPERATURE) return NS3D_ERR_INVALID_ARG;
     const int nq = what == NS3D_TEMPERATURE ? 1 : 5;
     for (int q = 0; q < nq; ++q) if (!out[q]) return NS3D_ERR_INVALID_ARG;
@@ -1191,6 +1370,10 @@ int ns3d_download(ns3d_handle *h, int what, double *const out[]) {
     double *const *scr = state_table(h, free_b);
     dim3 g = cell_grid(L, true, 128);
     if (what == NS3D_RHS) {
+        if (!h->rhs_complete)
+            return fail(h, NS3D_ERR_STATE,
+                        "the RHS buffer holds no complete right-hand side: an RK3 step's last stage stores "
+                        "it only when the handle was created with keep_rhs = 1 (else call ns3d_compute_rhs)");
         if (!h->mixed) {
             for (int q = 0; q < 5; ++q) if ((r = download_plane(h, out[q], h->rhs64[q], h->S[free_b][q]))) return r;
         } else {
@@ -1221,6 +1404,7 @@ int ns3d_download(ns3d_handle *h, int what, double *const out[]) {
 
 int ns3d_apply_boundary(ns3d_handle *h) {
     if (!h) return NS3D_ERR_INVALID_ARG;
+    h->prev_valid = false;  // the free state buffers are scratch here
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
     int r = set_device(h); if (r) return r;
     h->launches = 0;
@@ -1259,10 +1443,14 @@ int check_device_error(ns3d_handle *h) {
 int ns3d_rk3_step(ns3d_handle *h, double dt) {
     if (!h) return NS3D_ERR_INVALID_ARG;
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    if (is_slab(h))
+        return fail(h, NS3D_ERR_STATE, "a z-slab steps stage by stage (ns3d_rk3_stage) with a halo exchange between");
     if (!std::isfinite(dt)) return fail(h, NS3D_ERR_INVALID_ARG, "dt is not finite");
     int r = set_device(h); if (r) return r;
     h->launches = 0;
+    h->prev_valid = false;
     if ((r = rk3_async(h, dt))) return r;
+    h->prev_valid = true;
     if ((r = check_device_error(h))) return r;
     if (h->P.check_state) return check_state(h);
     return NS3D_OK;
@@ -1273,11 +1461,15 @@ int ns3d_rk3_step(ns3d_handle *h, double dt) {
 int ns3d_rk3_steps(ns3d_handle *h, int nsteps, double dt) {
     if (!h || nsteps < 0) return NS3D_ERR_INVALID_ARG;
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    if (is_slab(h))
+        return fail(h, NS3D_ERR_STATE, "a z-slab steps stage by stage (ns3d_rk3_stage) with a halo exchange between");
     if (!std::isfinite(dt)) return fail(h, NS3D_ERR_INVALID_ARG, "dt is not finite");
     int r = set_device(h); if (r) return r;
     h->launches = 0;
     for (int s = 0; s < nsteps; ++s) {
+        h->prev_valid = false;
         if ((r = rk3_async(h, dt))) return r;
+        h->prev_valid = true;
     }
     if ((r = check_device_error(h))) return r;
     if (h->P.check_state) return check_state(h);
@@ -1307,10 +1499,10 @@ int ns3d_compute_timestep(ns3d_handle *h, double *dt_out) {
     prof_begin(h, "cfl_dt");
     if (!h->mixed)
         dt_kernel64<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
-                                                                  h->ph.dx, h->partials);
+                                                                  h->ph.dx, h->partials, h->zlo, h->zhi - h->zlo);
     else
         dt_kernel_mixed<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
-                                                                      h->ph.dx, h->partials);
+                                                                      h->ph.dx, h->partials, h->zlo, h->zhi - h->zlo);
     prof_end(h);
     h->launches += 1;
     CK(h, cudaGetLastError(), "dt kernel");
@@ -1322,12 +1514,24 @@ int ns3d_compute_timestep(ns3d_handle *h, double *dt_out) {
 
 int ns3d_diagnostics(ns3d_handle *h, double out[6]) {
     if (!h || !out) return NS3D_ERR_INVALID_ARG;
+    h->prev_valid = false;  // the free state buffers are scratch here
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
     int r = set_device(h); if (r) return r;
     h->launches = 0;
     const double vol = h->ph.dx * h->ph.dy * h->ph.dz;
-    if (!h->mixed) {
-        diag_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(visc_args<double>(h), vol, h->partials);
+    double s[5];
+    if (!h->mixed && h->ph.mu != 0.0 && !h->diag_separate) {
+        // fused: the viscous kernel of the current state -- the one the next
+        // RK stage (or compute_rhs) starts with, which then reuses its node
+        // fluxes -- adds up the sums as it forms the gradients
+        long nb = 0;
+        if ((r = visc_launch<double>(h, h->visc_red, &nb))) return r;
+        h->visc_valid = true;
+        if ((r = reduce_combine(h, 5, 0, s, h->visc_red, nb))) return r;
+        if ((r = check_device_error(h))) return r;
+    } else if (!h->mixed) {
+        diag_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(visc_args<double>(h), vol, h->partials,
+                                                                           h->zlo, h->zhi - h->zlo);
     } else {
         // FP64 primitives of the current conserved state for the reductions
         const int b = (h->s0 + 1) % 3;
@@ -1342,14 +1546,15 @@ int ns3d_diagnostics(ns3d_handle *h, double out[6]) {
         for (int q = 0; q < 5; ++q) a.W[q] = h->S[b][q];
         a.T = h->S[bt][0];
         a.L = h->L64;
-        diag_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(a, vol, h->partials);
+        diag_kernel<double><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(a, vol, h->partials, h->zlo, h->zhi - h->zlo);
         h->launches += 1;
     }
-    h->launches += 1;
-    CK(h, cudaGetLastError(), "diagnostics");
-    double s[5];
-    if ((r = reduce_combine(h, 5, 0, s))) return r;
-    const double N = (double)h->G.nx * h->G.ny * h->G.nz;
+    if (h->mixed || h->ph.mu == 0.0 || h->diag_separate) {
+        h->launches += 1;
+        CK(h, cudaGetLastError(), "diagnostics");
+        if ((r = reduce_combine(h, 5, 0, s))) return r;
+    }
+    const double N = (double)h->G.nx * h->G.ny * (h->zhi - h->zlo);  // the owned cells
     const double mean_mu = s[2] / N, mean_rho = s[3] / N;
     out[0] = s[0];
     out[1] = s[1] / N;
@@ -1357,6 +1562,33 @@ int ns3d_diagnostics(ns3d_handle *h, double out[6]) {
     out[3] = mean_rho;
     out[4] = (mean_mu / mean_rho) * (s[1] / N);
     out[5] = std::sqrt(s[4] / (3.0 * N));
+    return NS3D_OK;
+}
+
+int ns3d_residuals(ns3d_handle *h, double out[5]) {
+    if (!h || !out) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    if (!h->prev_valid)
+        return fail(h, NS3D_ERR_STATE,
+                    "no step-start state to difference against: call right after an RK3 step or "
+                    "ns3d_time_advance, before any download or upload");
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    const int prev = (h->s0 + 2) % 3;
+    const double dx3 = h->ph.dx * h->ph.dx * h->ph.dx;  // compute_diagnostics weights by dx^3
+    if (!h->mixed)
+        residual_kernel<false><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(
+            state_table(h, h->s0), state_table(h, prev), h->L64, h->ph.gamma, dx3, h->partials, h->zlo, h->zhi - h->zlo);
+    else
+        residual_kernel<true><<<h->red_blocks, RED_THREADS, 0, h->stream>>>(
+            state_table(h, h->s0), state_table(h, prev), h->L64, h->ph.gamma, dx3, h->partials, h->zlo, h->zhi - h->zlo);
+    residual_combine_kernel<<<1, 32, 0, h->stream>>>(h->partials, h->red_blocks, h->scalars);
+    h->launches += 2;
+    CK(h, cudaGetLastError(), "residuals");
+    double v[10];
+    CK(h, cudaMemcpyAsync(v, h->scalars, sizeof(v), cudaMemcpyDeviceToHost, h->stream), "copy residuals");
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    for (int q = 0; q < 5; ++q) out[q] = std::sqrt(v[q]) / v[5 + q];
     return NS3D_OK;
 }
 
@@ -1396,10 +1628,10 @@ int seed_cfl_min(ns3d_handle *h) {
         min_combine_kernel<<<h->red_blocks, 256, 0, h->stream>>>(h->cfl_part, h->cfl_count, h->partials);
     } else if (!h->mixed) {
         dt_kernel64<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
-                                                                  h->ph.dx, h->partials);
+                                                                  h->ph.dx, h->partials, h->zlo, h->zhi - h->zlo);
     } else {
         dt_kernel_mixed<<<h->red_blocks, RED_THREADS, 0, h->stream>>>(state_table(h, h->s0), h->L64, h->ph.gamma,
-                                                                      h->ph.dx, h->partials);
+                                                                      h->ph.dx, h->partials, h->zlo, h->zhi - h->zlo);
     }
     min_combine_kernel<<<1, 256, 0, h->stream>>>(h->partials, h->red_blocks, &h->clock->cfl_min);
     h->launches += 2;
@@ -1419,6 +1651,7 @@ int capture_adv_graph(ns3d_handle *h, int li, int s0) {
     CK(h, cudaStreamSynchronize(h->stream), "synchronize");
     const int keep = h->s0;
     const bool keep_valid = h->cfl_valid;  // capturing executes nothing: the stored minima stay as they were
+    const bool keep_rhs_flag = h->rhs_complete, keep_visc = h->visc_valid;
     h->s0 = s0;
     h->dev_loop = true;
     cudaGraph_t g = nullptr;
@@ -1439,6 +1672,8 @@ int capture_adv_graph(ns3d_handle *h, int li, int s0) {
     h->dev_loop = false;
     h->s0 = keep;
     h->cfl_valid = keep_valid;
+    h->rhs_complete = keep_rhs_flag;
+    h->visc_valid = keep_visc;
     if (r == NS3D_OK && e == cudaSuccess) e = cudaGraphInstantiate(&h->adv_graph[li][s0], g, 0);
     if (g) cudaGraphDestroy(g);
     if (r != NS3D_OK) return r;
@@ -1472,7 +1707,12 @@ int time_advance_device(ns3d_handle *h, double t_end, int max_steps, double *tim
         const int ran = c.steps - total;  // steps this launch executed (the rest returned at once)
         total = c.steps;
         h->s0 = (s0 + ran) % 3;
-        if (ran > 0) h->cfl_valid = true;
+        if (ran > 0) {
+            h->visc_valid = false;
+            h->cfl_valid = true;
+            h->rhs_complete = h->P.keep_rhs != 0;
+            h->prev_valid = true;
+        }
         if ((r = check_device_error(h))) break;
         if (c.err) { r = fail(h, NS3D_ERR_DT, "dt too small or zero"); break; }
         if (h->P.check_state && ran > 0 && (r = check_state(h))) break;
@@ -1486,6 +1726,8 @@ int time_advance_device(ns3d_handle *h, double t_end, int max_steps, double *tim
 int ns3d_time_advance(ns3d_handle *h, double t_end, int max_steps, double *time, int *steps_done) {
     if (!h || !time) return NS3D_ERR_INVALID_ARG;
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    if (is_slab(h))
+        return fail(h, NS3D_ERR_STATE, "a z-slab steps stage by stage (ns3d_rk3_stage) with a halo exchange between");
     // per-kernel event profiling cannot sit inside a captured graph
     if (!h->profiling && max_steps > 0) return time_advance_device(h, t_end, max_steps, time, steps_done);
     const double eps = 1e-12;
@@ -1507,6 +1749,61 @@ int ns3d_time_advance(ns3d_handle *h, double t_end, int max_steps, double *time,
     return r;
 }
 
+int ns3d_set_slab(ns3d_handle *h, int z_begin, int z_end, double dz) {
+    if (!h || z_begin < 0 || z_end > h->G.nz || z_end - z_begin < 1) return NS3D_ERR_INVALID_ARG;
+    if (!(dz > 0.0) && dz != 0.0) return NS3D_ERR_INVALID_ARG;
+    const bool slab = z_begin != 0 || z_end != h->G.nz;
+    if (slab && ((z_begin != 0 && z_begin < 6) || (z_end != h->G.nz && h->G.nz - z_end < 6) || z_end - z_begin < 6))
+        return fail(h, NS3D_ERR_INVALID_ARG, "a z-slab needs six halo planes on each bordering side and six owned planes");
+    if (slab && h->bc.periodic[2])
+        return fail(h, NS3D_ERR_CONFIG, "a z-slab's local z boundaries are its halos: give them a non-periodic type");
+    int r = set_device(h); if (r) return r;
+    CK(h, cudaStreamSynchronize(h->stream), "synchronize");
+    // captured time-advance graphs hold the old launch geometry
+    for (auto &row : h->adv_graph)
+        for (auto &g : row)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    h->zlo = z_begin;
+    h->zhi = z_end;
+    h->visc_valid = false;
+    if (dz > 0.0) { h->ph.dz = dz; h->ph.inv_dz = 1.0 / dz; }
+    h->cfl_valid = false;
+    h->prev_valid = false;
+    h->step_start = -1;
+    return NS3D_OK;
+}
+
+int ns3d_rk3_stage(ns3d_handle *h, int stage, double dt) {
+    if (!h || stage < 1 || stage > 3) return NS3D_ERR_INVALID_ARG;
+    if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
+    if (!std::isfinite(dt)) return fail(h, NS3D_ERR_INVALID_ARG, "dt is not finite");
+    if (stage != 1 && (h->step_start < 0 || h->s0 != (h->step_start + stage - 1) % 3))
+        return fail(h, NS3D_ERR_STATE, "RK3 stages run in order 1, 2, 3");
+    int r = set_device(h); if (r) return r;
+    h->launches = 0;
+    if (stage == 1) {
+        h->prev_valid = false;
+        h->step_start = h->s0;
+    }
+    // rk3_async's buffers: (1: s0, s0 -> b1), (2: s0, b1 -> b2), (3: s0, b2 -> b1)
+    const int s0 = h->step_start, b1 = (s0 + 1) % 3, b2 = (s0 + 2) % 3;
+    const int srcc = stage == 1 ? s0 : (stage == 2 ? b1 : b2);
+    const int dst = stage == 2 ? b2 : b1;
+    if ((r = rk_stage_async(h, stage, s0, srcc, dst, dt))) {
+        h->s0 = s0;
+        h->step_start = -1;
+        return r;
+    }
+    h->s0 = dst;
+    if (stage == 3) {
+        h->step_start = -1;
+        h->prev_valid = true;
+        if ((r = check_device_error(h))) return r;
+        if (h->P.check_state) return check_state(h);
+    }
+    return NS3D_OK;
+}
+
 int ns3d_device_fields(ns3d_handle *h, int what, void *ptrs[5], long layout[6]) {
     if (!h || !ptrs || !layout) return NS3D_ERR_INVALID_ARG;
     const Layout *L = &h->L64;
@@ -1521,6 +1818,10 @@ int ns3d_device_fields(ns3d_handle *h, int what, void *ptrs[5], long layout[6]) 
     } else if (what == NS3D_RHS) {
         for (int q = 0; q < 5; ++q) ptrs[q] = h->mixed ? (void *)h->rhs32[q] : (void *)h->rhs64[q];
         if (h->mixed) { L = &h->L32; esz = 4; }
+    } else if (what == NS3D_TEMPERATURE) {
+        ptrs[0] = h->mixed ? (void *)h->T32 : (void *)h->T64;
+        for (int q = 1; q < 5; ++q) ptrs[q] = nullptr;
+        if (h->mixed) { L = &h->L32; esz = 4; }
     } else {
         return fail(h, NS3D_ERR_INVALID_ARG, "group not resident on the device in this precision");
     }
@@ -1530,6 +1831,8 @@ int ns3d_device_fields(ns3d_handle *h, int what, void *ptrs[5], long layout[6]) 
 
 int ns3d_vjp_rhs(ns3d_handle *h, const double *const rbar[5], double *const ubar[5]) {
     if (!h || !rbar || !ubar) return NS3D_ERR_INVALID_ARG;
+    h->visc_valid = false;
+    h->prev_valid = false;  // the free state buffers are scratch here
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
     std::string why;
     if (!adjoint_supported(h, why)) return fail(h, NS3D_ERR_CONFIG, why);
@@ -1544,6 +1847,8 @@ int ns3d_vjp_rhs(ns3d_handle *h, const double *const rbar[5], double *const ubar
 
 int ns3d_vjp_rk3_step(ns3d_handle *h, double dt, const double *const ubar_next[5], double *const ubar[5]) {
     if (!h || !ubar_next || !ubar) return NS3D_ERR_INVALID_ARG;
+    h->visc_valid = false;
+    h->prev_valid = false;  // the free state buffers are scratch here
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
     std::string why;
     if (!adjoint_supported(h, why)) return fail(h, NS3D_ERR_CONFIG, why);
@@ -1577,6 +1882,8 @@ int ns3d_vjp_rk3_step(ns3d_handle *h, double dt, const double *const ubar_next[5
 int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int checkpoint_every, double *J,
                                 double *const grad[3], double stats[4]) {
     if (!h || !J || !grad || nsteps < 1 || checkpoint_every < 1) return NS3D_ERR_INVALID_ARG;
+    h->visc_valid = false;
+    h->prev_valid = false;
     if (!h->has_state) return fail(h, NS3D_ERR_STATE, "no state uploaded");
     std::string why;
     if (!adjoint_supported(h, why)) return fail(h, NS3D_ERR_CONFIG, why);

@@ -32,6 +32,59 @@ __device__ __forceinline__ void block_sum(double v[NV], double *partial_out) {
     }
 }
 
+// Sums of v[0..NV) over a block of NT threads of any shape (NT a multiple of
+// 32, every thread calling), in a fixed order; thread 0 writes them.
+template <int NV, int NT>
+__device__ __forceinline__ void block_sum_n(double v[NV], double *out) {
+    __shared__ double sh[NV][NT / 32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double x = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[q][wid] = x;
+    }
+    __syncthreads();
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = 0.0;
+            for (int w = 0; w < NT / 32; ++w) s += sh[q][w];
+            out[q] = s;
+        }
+    }
+}
+
+// Sums of s[0..NV) and maxima of m[0..NV) over a block of RED_THREADS
+// threads, in a fixed order; thread 0 writes s then m (2 NV values).
+template <int NV>
+__device__ __forceinline__ void block_sum_max(double s[NV], double m[NV], double *partial_out) {
+    __shared__ double sh[2 * NV][RED_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double x = s[q], y = m[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            x += __shfl_down_sync(0xffffffffu, x, o);
+            y = fmax(y, __shfl_down_sync(0xffffffffu, y, o));
+        }
+        if (lane == 0) { sh[q][wid] = x; sh[NV + q][wid] = y; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double a = 0.0, b = 0.0;
+            for (int w = 0; w < RED_THREADS / 32; ++w) { a += sh[q][w]; b = fmax(b, sh[NV + q][w]); }
+            partial_out[q] = a;
+            partial_out[NV + q] = b;
+        }
+    }
+}
+
 __device__ __forceinline__ double block_min(double x, double *partial_out) {
     __shared__ double sh[RED_THREADS / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;

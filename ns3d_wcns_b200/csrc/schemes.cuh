@@ -97,12 +97,36 @@ NS3D_HD float mdcd_beta3(float f0, float f1, float f2, float f3, float f4, float
 // right state swaps a_j and b_j of the same two points with the same
 // operation order, so both states of a face take the same decision:
 // smooth(cell i) && smooth(cell i+1) for the face i+1/2.
+//
+// The detector is the one discontinuous decision of the scheme, so the FP64
+// build takes the reference's decision exactly: the cross-multiplied test
+// (whose products the compiler may fuse) decides every case farther than
+// 1e-12 relative from the threshold -- far beyond its few-ulp rounding -- and
+// the rest are decided by the reference's own quotient, term by term with
+// unfused IEEE operations (mdcd_sai_ref).  a and b themselves round as in the
+// reference: 2 f is exact, so a fused f0 - 2 fm1 gives the same bits.
+NS3D_HD double mdcd_sai_ref(double a, double b) {
+    const double eps = 0.9 * 0.4 / (1.0 - 0.9 * 0.4) * 1e-4;
+#ifdef __CUDA_ARCH__
+    const double num = __dadd_rn(__dmul_rn(__dmul_rn(2.0, a), b), eps);
+    const double den = __dadd_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)), eps);
+    return __ddiv_rn(num, den);
+#else
+    volatile double aa = a * a, bb = b * b, ab2 = 2.0 * a * b;
+    return (ab2 + eps) / (aa + bb + eps);
+#endif
+}
+
 template <typename R>
 NS3D_HD bool mdcd_smooth(R fm2, R fm1, R f0, R fp1, R fp2) {
     const R eps = R(0.9 * 0.4 / (1.0 - 0.9 * 0.4) * 1e-4);
     R a = fabs(f0 - fm1) + fabs(f0 - R(2) * fm1 + fm2);
     R b = fabs(f0 - fp1) + fabs(f0 - R(2) * fp1 + fp2);
-    return (R(2) * a * b + eps) > R(0.4) * (a * a + b * b + eps);
+    const R lhs = R(2) * a * b + eps, rhs = R(0.4) * (a * a + b * b + eps);
+    if constexpr (sizeof(R) == 8) {
+        if (fabs(lhs - rhs) <= 1e-12 * rhs) return mdcd_sai_ref(a, b) > 0.4;
+    }
+    return lhs > rhs;
 }
 
 // The non-linear branch: 4-stencil WENO with weights d_k (20 + tau6/(beta_k +

@@ -65,6 +65,7 @@ struct FusedStage {
     const double *dt_dev;   // non-null: dt from the device time loop
     double gamma, Rgas, dx, vol;
     double *cfl_part, *ke_part;  // stage 3: per-block CFL minimum and kinetic energy
+    int keep_rhs;                // also write the complete RHS (the handle's keep_rhs, stage 3 only)
 };
 
 template <typename R>
@@ -82,6 +83,8 @@ struct SweepArgs {
     int first;          // 1: write (first direction), 0: accumulate
     int visc;           // 1: add the viscous divergence term
     const int *done;    // non-null: skip the launch while *done (device time loop)
+    int zlo, zhi;       // owned interior z-planes [zlo, zhi): the x/y sweeps run over them, the
+                        // z-sweep updates only them (the rest of a z-slab's planes are halo)
     FusedStage fs;      // z-sweep only
 };
 
@@ -215,7 +218,7 @@ sweep_kernel(SweepArgs<R> a) {
     float def_w[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, def_t = 0.f;
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int line = DIR == 0 ? threadIdx.y : threadIdx.x;
-    const int ta0 = blockIdx.x * NL + line, tb0 = blockIdx.y;
+    const int ta0 = blockIdx.x * NL + line, tb0 = blockIdx.y + (DIR == 2 ? 0 : a.zlo);
     const bool line_ok = ta0 < (DIR == 0 ? L.ny : L.nx);
     const int n = DIR == 0 ? L.nx : (DIR == 1 ? L.ny : L.nz);
     // padded-layout address of cell c (ghost-inclusive index along the line)
@@ -295,7 +298,7 @@ sweep_kernel(SweepArgs<R> a) {
         // cell updated by this thread in this chunk; its old RHS (plain
         // loads, consumed after the face phase)
         const int cu = fc - 2 + slot;
-        const bool upd = line_ok && cu >= NG && cu < n + NG;
+        const bool upd = line_ok && cu >= NG && cu < n + NG && (DIR != 2 || (cu - NG >= a.zlo && cu - NG < a.zhi));
         const long cid = lbase + cu * lstride;
         R rold[5];
 #pragma unroll
@@ -633,7 +636,7 @@ sweep_kernel(SweepArgs<R> a) {
                     fused = true;
                 }
             }
-            if (!fused) {
+            if (!fused || a.fs.keep_rhs) {  // keep_rhs: the last stage's complete RHS as well
 #pragma unroll
                 for (int q = 0; q < 5; ++q) a.Rhs[q][cid] = rq[q];
             }
@@ -690,8 +693,8 @@ inline cudaError_t launch_sweep(const SweepArgs<R> &a, cudaStream_t st) {
     using G = SweepGeom<DIR>;
     dim3 block(DIR == 0 ? G::C : G::NLINE, DIR == 0 ? G::NLINE : G::C);
     dim3 grid;
-    if (DIR == 0) grid = dim3((a.L.ny + G::NLINE - 1) / G::NLINE, a.L.nz);
-    else if (DIR == 1) grid = dim3((a.L.nx + G::NLINE - 1) / G::NLINE, a.L.nz);
+    if (DIR == 0) grid = dim3((a.L.ny + G::NLINE - 1) / G::NLINE, a.zhi - a.zlo);
+    else if (DIR == 1) grid = dim3((a.L.nx + G::NLINE - 1) / G::NLINE, a.zhi - a.zlo);
     else grid = dim3((a.L.nx + G::NLINE - 1) / G::NLINE, a.L.ny);
     const size_t smem = sweep_smem_bytes<DIR, R, CHAR != 0>();
     static unsigned configured = 0;  // one bit per device ordinal

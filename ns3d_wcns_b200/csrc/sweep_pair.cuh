@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
     bool has_def = false;
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int pr = DIR == 0 ? threadIdx.y : threadIdx.x;
-    const int ta0 = blockIdx.x * NL + 2 * pr, tb0 = blockIdx.y;  // first line of the pair
+    const int ta0 = blockIdx.x * NL + 2 * pr, tb0 = blockIdx.y + (DIR == 2 ? 0 : a.zlo);  // first line of the pair
     const bool line_ok = ta0 < (DIR == 0 ? L.ny : L.nx);          // both lines (even count)
     const int n = DIR == 0 ? L.nx : (DIR == 1 ? L.ny : L.nz);
     // padded-layout address of cell c of the first line; the second line is
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
     for (int fc = fb; fc < chunk_end; fc += C) {
         // cell updated by this thread (both lines) in this chunk
         const int cu = fc - 2 + slot;
-        const bool upd = line_ok && cu >= NG && cu < n + NG;
+        const bool upd = line_ok && cu >= NG && cu < n + NG && (DIR != 2 || (cu - NG >= a.zlo && cu - NG < a.zhi));
         const long cid = lbase + cu * lstride;
         if (rmw && upd) {
 #pragma unroll
@@ -579,7 +579,7 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
                     fused = true;
                 }
             }
-            if (!fused) {
+            if (!fused || a.fs.keep_rhs) {  // keep_rhs: the last stage's complete RHS as well
 #pragma unroll
                 for (int q = 0; q < 5; ++q) st2(a.Rhs[q] + cid, lpair, rq[q]);
             }
@@ -637,7 +637,7 @@ template <int DIR, int INTERP, int RS>
 inline cudaError_t launch_pair(const SweepArgs<float> &a, cudaStream_t st) {
     using G = PairGeom<DIR>;
     dim3 block(DIR == 0 ? G::C : G::NP, DIR == 0 ? G::NP : G::C);
-    dim3 grid(((DIR == 0 ? a.L.ny : a.L.nx) + G::NL - 1) / G::NL, DIR == 2 ? a.L.ny : a.L.nz);
+    dim3 grid(((DIR == 0 ? a.L.ny : a.L.nx) + G::NL - 1) / G::NL, DIR == 2 ? a.L.ny : a.zhi - a.zlo);
     const size_t smem = pair_smem_bytes<DIR>();
     static unsigned configured = 0;  // one bit per device ordinal
     int dev = 0;

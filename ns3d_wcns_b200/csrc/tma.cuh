@@ -60,6 +60,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
     return false;
 }
 
+// After a timed-out wait: the copies already issued may still land in this
+// block's shared memory, so the block waits for them (bounded by a longer
+// limit) before it retires, and issues nothing more.
+constexpr unsigned TMA_DRAIN_LIMIT = 1u << 26;
+__device__ __forceinline__ bool mbar_drain(uint64_t *bar, unsigned parity) {
+    for (unsigned it = 0; it < TMA_DRAIN_LIMIT; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 // order this thread's earlier generic-proxy shared-memory accesses before
 // later async-proxy (TMA) writes to the same memory
 __device__ __forceinline__ void fence_proxy_async_smem() {

@@ -21,6 +21,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "reduce.cuh"
 #include "tma.cuh"
 
 namespace ns3d {
@@ -37,6 +38,13 @@ struct ViscArgs {
     R mu0, S, cp_over_pr;
     int *err;               // device error word (a bounded wait that ran out)
     const int *done;        // non-null: skip the launch while *done (device time loop)
+    int zlo, zhi;           // interior z-planes whose node fluxes are computed
+    // non-null: also the turbulence sums of ns3d_diagnostics over the nodes of
+    // planes [rlo, rhi), five per block in the order of diag_kernel:
+    // 0.5 rho |u|^2 vol, sum_ij (du_i/dx_j)^2, mu(T), rho, |u|^2
+    double *red;
+    int rlo, rhi;
+    double vol;
 };
 
 // choose_scheme, ViscousFlux.cpp:33-50 (idx relative to the first interior node)
@@ -126,7 +134,7 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
     if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
     const int x0 = blockIdx.x * VTX, y0 = blockIdx.y * VTY;
-    const int kb = blockIdx.z * VZC, ke = min(kb + VZC, L.nz);
+    const int kb = a.zlo + blockIdx.z * VZC, ke = min(kb + VZC, a.zhi);
     const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
     const int tid = threadIdx.y * VTX + threadIdx.x;
     const bool in = i < L.nx && j < L.ny;
@@ -150,6 +158,7 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
     };
     unsigned phase = 0u;  // bit b: parity of buffer b's next completion
     if (tid == 0) issue(0, kb);
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ns3d_diagnostics sums (a.red)
     // window: win[q][m] = value at interior plane k - 3 + m (ghost-inclusive k + m)
     R win[4][7], nxt[4];
 #pragma unroll
@@ -172,11 +181,18 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
 #pragma unroll
             for (int q = 0; q < 4; ++q) nxt[q] = src[q][col + (long)(k + 7) * zs];
         }
-        const bool ok = mbar_wait_bounded(&bar[buf], (phase >> buf) & 1u, a.err);
+        const unsigned par = (phase >> buf) & 1u;
+        const bool ok = mbar_wait_bounded(&bar[buf], par, a.err);
         phase ^= 1u << buf;
         if (__syncthreads_or(!ok)) {
-            // a tile never arrived: let the other copy (if any) land, bounded, and stop
-            if (more && tid == 0) mbar_wait_bounded(&bar[buf ^ 1], (phase >> (buf ^ 1)) & 1u, a.err);
+            // a tile did not arrive in time (the error word is set): issue
+            // nothing more, and let both copies in flight land (bounded)
+            // before the block retires
+            if (tid == 0) {
+                mbar_drain(&bar[buf], par);
+                if (more) mbar_drain(&bar[buf ^ 1], (phase >> (buf ^ 1)) & 1u);
+            }
+            __syncthreads();
             return;
         }
         if (in) {
@@ -207,6 +223,20 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
             a.V[6][o] = u * txx + v * txy + w * txz + kq * Tx;
             a.V[7][o] = u * txy + v * tyy + w * tyz + kq * Ty;
             a.V[8][o] = u * txz + v * tyz + w * tzz + kq * Tz;
+            if (a.red && k >= a.rlo && k < a.rhi) {
+                const double rho = (double)a.W[0][col + (long)(k + NG) * zs];
+                const double du = u, dv = v, dw = w, uu = du * du + dv * dv + dw * dw;
+                acc[0] += 0.5 * rho * uu * a.vol;
+                double g2 = 0.0;
+#pragma unroll
+                for (int q = 0; q < 3; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) g2 += (double)g[q][d] * (double)g[q][d];
+                acc[1] += g2;
+                acc[2] += (double)mu;
+                acc[3] += rho;
+                acc[4] += uu;
+            }
         }
 #pragma unroll
         for (int m = 0; m < 6; ++m)
@@ -214,6 +244,8 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
             for (int q = 0; q < 4; ++q) win[q][m] = win[q][m + 1];
         __syncthreads();  // this tile's reads done before it is refilled
     }
+    if (a.red)  // uniform: every thread of the block arrives
+        block_sum_n<5, VTX * VTY>(acc, a.red + 5 * ((long)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x));
 }
 
 // All 12 derivatives at interior node (i,j,k) (ghost-inclusive indices), for

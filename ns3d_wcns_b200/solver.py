@@ -26,7 +26,7 @@ PRIMITIVE = ("rho", "u", "v", "w", "p")
 RHS = ("rhs_rho", "rhs_rhou", "rhs_rhov", "rhs_rhow", "rhs_E")
 
 
-def _params(P: SolverParams, device: int, check_state: bool) -> _lib.Params:
+def _params(P: SolverParams, device: int, check_state: bool, keep_rhs: bool = False) -> _lib.Params:
     lib = _lib.load()
     p = _lib.Params()
     lib.ns3d_params_default(C.byref(p))
@@ -39,19 +39,21 @@ def _params(P: SolverParams, device: int, check_state: bool) -> _lib.Params:
     p.precision = int(P.precision)
     p.device = device
     p.check_state = int(check_state)
+    p.keep_rhs = int(keep_rhs)
     return p
 
 
 class Solver:
     """One GPU-resident ns3d_wcns state (whole domain on one device)."""
 
-    def __init__(self, P: SolverParams, G: GridDesc, device: int = 0, check_state: bool = False):
+    def __init__(self, P: SolverParams, G: GridDesc, device: int = 0, check_state: bool = False,
+                 keep_rhs: bool = False):
         self.lib = _lib.load()
         self.P, self.G = P, G
         self.device = device
         grid = _lib.Grid(G.global_nx, G.global_ny, G.global_nz, G.x0, G.y0, G.z0, G.Lx, G.Ly, G.Lz)
         h = C.c_void_p()
-        r = self.lib.ns3d_create(C.byref(_params(P, device, check_state)), C.byref(grid), C.byref(h))
+        r = self.lib.ns3d_create(C.byref(_params(P, device, check_state, keep_rhs)), C.byref(grid), C.byref(h))
         if r != 0:
             raise _lib.Ns3dError(r, self.lib.ns3d_last_error(None).decode() or
                                  self.lib.ns3d_status_string(r).decode())
@@ -108,6 +110,13 @@ class Solver:
                 raise ValueError("expected interior-sized arrays")
         self._check(self.lib.ns3d_set_interior_primitives(self.h, self._ptrs(arrs)))
 
+    INIT_KINDS = {"riemann_2d": 0, "sod": 1, "uniform": 2, "sine_x": 3}
+
+    def initialize(self, kind: str) -> None:
+        """One of the reference's built-in initialisers on the device, then the
+        ghost fill (main.cpp:85-99): riemann_2d, sod, uniform or sine_x."""
+        self._check(self.lib.ns3d_initialize(self.h, self.INIT_KINDS[kind]))
+
     def download(self, what: int) -> np.ndarray:
         nq = 1 if what == _lib.NS3D_TEMPERATURE else 5
         out = np.empty((nq,) + self.shape, dtype=np.float64)
@@ -126,6 +135,12 @@ class Solver:
 
     def rk3_steps(self, nsteps: int, dt: float) -> None:
         self._check(self.lib.ns3d_rk3_steps(self.h, int(nsteps), C.c_double(dt)))
+
+    def residuals(self) -> np.ndarray:
+        """compute_diagnostics' residual norms of the last step (F.global_res_rho ... F.global_res_E)."""
+        out = (C.c_double * 5)()
+        self._check(self.lib.ns3d_residuals(self.h, out))
+        return np.array(list(out))
 
     def compute_timestep(self) -> float:
         x = C.c_double()

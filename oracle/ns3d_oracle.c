@@ -978,6 +978,29 @@ double orc_total_energy(void) {
     return sum;
 }
 
+/* compute_diagnostics, postprocess.cpp:7-98, with updateResiduals
+ * (field_structures.h:500-508): per conserved variable sqrt(sum over the
+ * interior of (U - U0)^2 dx^3) / max |U|, U0 the state recorded at the start
+ * of the last step (orc_rk3_step).  Same loop and operation order. */
+void orc_residuals(double out[5]) {
+    const double dx3 = S->dx * S->dx * S->dx;
+    double sq[5] = {0, 0, 0, 0, 0}, mx[5] = {0, 0, 0, 0, 0};
+    for (int k = NG; k < NG + S->nz; ++k)
+        for (int j = NG; j < NG + S->ny; ++j)
+            for (int i = NG; i < NG + S->nx; ++i) {
+                long id = I3(i, j, k);
+                for (int n = 0; n < 5; ++n) {
+                    double a = fabs(S->U[n][id]);
+                    mx[n] = mx[n] < a ? a : mx[n];  /* std::max(max_abs, |x|) */
+                }
+                for (int n = 0; n < 5; ++n) {
+                    double r = S->U[n][id] - S->U0[n][id];
+                    sq[n] += r * r * dx3;
+                }
+            }
+    for (int n = 0; n < 5; ++n) out[n] = sqrt(sq[n]) / mx[n];
+}
+
 /* main.cpp:98-99 after an initialiser: interior primitives -> ghosts -> conserved. */
 int orc_set_interior_prims(const double *rho, const double *u, const double *v, const double *w,
                            const double *p) {

@@ -48,6 +48,7 @@ void orc_cons_to_prim(void);
 void orc_rk3_step(double dt);
 double orc_timestep(void);
 double orc_total_energy(void);
+void orc_residuals(double out[5]);
 
 /* Scalar kernels, exported for known-answer tests against the reference. */
 double orc_weno5(const double f[6]);

@@ -23,7 +23,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "_build", "libns3d_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libns3d_ref.so")
 DROPIN_LIB = os.path.join(HERE, "_ref", "libns3d_dropin.so")
-REF_SRC_DIR = "/root/reference"
+DROPIN_LOOP_LIB = os.path.join(HERE, "_ref", "libns3d_dropin_loop.so")
+# The reference sources (a checkout of ns3d_wcns): NS3D_REF_DIR, else a
+# checkout named "reference" beside this repository.  Only the build of the
+# test oracle reads them.
+REF_SRC_DIR = os.path.abspath(os.environ.get("NS3D_REF_DIR") or
+                              os.path.join(HERE, os.pardir, os.pardir, "reference"))
 
 _dp = C.POINTER(C.c_double)
 
@@ -117,6 +122,7 @@ class PortSolver(_Base):
         lib.orc_rk3_step.argtypes = [C.c_double]
         lib.orc_timestep.restype = C.c_double
         lib.orc_total_energy.restype = C.c_double
+        lib.orc_residuals.argtypes = [_dp]
         lib.orc_weno5.restype = C.c_double
         lib.orc_weno5.argtypes = [_dp]
         lib.orc_mdcd_linear.restype = C.c_double
@@ -147,6 +153,11 @@ class PortSolver(_Base):
     def timestep(self) -> float: return self.lib.orc_timestep()
     def total_energy(self) -> float: return self.lib.orc_total_energy()
 
+    def residuals(self) -> np.ndarray:
+        out = np.zeros(5)
+        self.lib.orc_residuals(_ptr(out))
+        return out
+
 
 class RefSolver(_Base):
     """The reference sources compiled in place (oracle/_ref/libns3d_ref.so)."""
@@ -164,6 +175,8 @@ class RefSolver(_Base):
         lib.ref_timestep.restype = C.c_double
         lib.ref_total_energy.restype = C.c_double
         lib.ref_params.argtypes = [_dp, C.POINTER(C.c_int)]
+        lib.ref_residuals.argtypes = [_dp]
+        lib.ref_monitor_values.argtypes = [_dp]
         self.lib = lib
         text = solver_in_text if solver_in_text is not None else format_solver_in(P, G)
         with tempfile.NamedTemporaryFile("w", suffix=".in", delete=False) as f:
@@ -191,6 +204,23 @@ class RefSolver(_Base):
     def timestep(self) -> float: return self.lib.ref_timestep()
     def total_energy(self) -> float: return self.lib.ref_total_energy()
     def time_advance(self): self.lib.ref_time_advance()
+
+    def residuals(self) -> np.ndarray:
+        out = np.zeros(5)
+        self.lib.ref_residuals(_ptr(out))
+        return out
+
+    def initialize(self, kind: str) -> None:
+        """initialize_riemann_2d / _sod_shock_tube / _uniform_field / _sine_x_field + ghost fill."""
+        r = self.lib.ref_initialize({"riemann_2d": 0, "sod": 1, "uniform": 2, "sine_x": 3}[kind])
+        if r != 0:
+            raise RuntimeError("ref_initialize failed")
+
+    def monitor_values(self) -> np.ndarray:
+        """F.global_Etot, F.global_res_rho ... F.global_res_E after time_advance."""
+        out = np.zeros(6)
+        self.lib.ref_monitor_values(_ptr(out))
+        return out
 
 
 def _kat_lib(path):

@@ -170,6 +170,39 @@ double ref_total_energy(void) {
     return S->F.global_Etot;
 }
 
+/* One of the reference's built-in initialisers (initialization.cpp:516-638),
+ * then apply_boundary + primitiveToConserved as main.cpp:85-99.  kind: 0
+ * riemann_2d, 1 sod, 2 uniform, 3 sine_x. */
+int ref_initialize(int kind) {
+    if (!S) return -1;
+    switch (kind) {
+        case 0: initialize_riemann_2d(S->F, S->G, S->P); break;
+        case 1: initialize_sod_shock_tube(S->F, S->G, S->P); break;
+        case 2: initialize_uniform_field(S->F, S->G, S->P); break;
+        case 3: initialize_sine_x_field(S->F, S->G, S->P); break;
+        default: return -1;
+    }
+    apply_boundary(S->F, S->G, S->C, S->P);
+    S->F.primitiveToConserved(S->P);
+    return 0;
+}
+
+/* compute_diagnostics (postprocess.cpp:7-98) after the last step: the
+ * residual norms F.global_res_rho ... F.global_res_E. */
+void ref_residuals(double *out5) {
+    compute_diagnostics(S->F, S->P, S->G);
+    const Field3D &F = S->F;
+    out5[0] = F.global_res_rho; out5[1] = F.global_res_rhou; out5[2] = F.global_res_rhov;
+    out5[3] = F.global_res_rhow; out5[4] = F.global_res_E;
+}
+
+/* F.global_Etot and the residual norms as the last time_advance left them. */
+void ref_monitor_values(double *out6) {
+    const Field3D &F = S->F;
+    out6[0] = F.global_Etot; out6[1] = F.global_res_rho; out6[2] = F.global_res_rhou;
+    out6[3] = F.global_res_rhov; out6[4] = F.global_res_rhow; out6[5] = F.global_res_E;
+}
+
 /* The reference's own step loop (maincycle.cpp:7-113) with the run-control
  * keys of the parsed solver.in; output writers are no-ops. */
 void ref_time_advance(void) { time_advance(S->F, S->C, S->G, S->P); }

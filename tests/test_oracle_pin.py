@@ -78,3 +78,5 @@ def test_port_matches_reference_live(interp, rs, ch, bcs):
         b.rk3_step(2e-4)
     assert np.array_equal(a.conserved(), b.conserved())
     assert np.array_equal(a.rhs(), b.rhs())
+    # compute_diagnostics' residual norms of the last step
+    assert np.array_equal(a.residuals(), b.residuals())

@@ -166,3 +166,78 @@ def test_cfl_fused_into_last_stage(gpu_lib, precision, bcs):
             # kinetic energy: the same sum in another (fixed) order
             ke_plain = s.total_energy()
             assert abs(ke_fused - ke_plain) <= 1e-13 * abs(ke_plain), (ke_fused, ke_plain)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_rhs_after_step_kept_on_request(gpu_lib, precision):
+    """runge_kutta_3 leaves its last stage's right-hand side in F.rhs_*
+    (range_kutta.cpp:80-88).  With keep_rhs the fused last stage stores it
+    too; without it the RHS buffer holds a partial sum after a step, and its
+    download is refused rather than handing that back.  FP64: relative
+    L-infinity 1e-12 against the oracle; mixed (continuous MDCD_LINEAR, so
+    no detector flips): relative L2 1e-4 per variable."""
+    from ns3d_wcns_b200 import _lib
+    from ns3d_wcns_b200 import analysis
+    from ns3d_wcns_b200.solver import Solver
+    n = (12, 10, 8)
+    interp = 3 if precision == 0 else 2
+    kw = dict(n=n, L=(1.0, 0.8, 0.7), interpolation=interp, riemann=2, bcs=(3, 3, 0, 0, 1, 2))
+    P, G = make_params(precision=precision, **kw)
+    st = random_state(n, seed=6, amp=0.2)
+    o = oracle.PortSolver(make_params(**kw)[0], G)
+    o.set_interior_prims(*st)
+    for _ in range(2):
+        o.rk3_step(3e-4)
+    with Solver(P, G, keep_rhs=True) as s:
+        s.set_interior_primitives(*st)
+        s.rk3_steps(2, 3e-4)
+        got, ref = interior(s.rhs()), interior(o.rhs())
+        if precision == 0:
+            err = per_var(got, ref)
+            assert err <= RHS_TOL, err
+        else:
+            err = max(analysis.rel_l2(a, b) for a, b in zip(got, ref))
+            assert err <= 1e-4, err
+        # the device time loop keeps it as well
+        t, k = s.time_advance(1.0, 1)
+        assert k == 1
+        s.rhs()
+    with Solver(P, G) as s:
+        s.set_interior_primitives(*st)
+        s.rk3_step(3e-4)
+        with pytest.raises(_lib.Ns3dError) as e:
+            s.rhs()
+        assert e.value.status == -7
+        s.compute_rhs()
+        s.rhs()
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference not built")
+@pytest.mark.parametrize("kind", ["riemann_2d", "sod", "uniform", "sine_x"])
+@pytest.mark.parametrize("bcs", [(0,) * 6, (3, 3, 1, 2, 0, 0)])
+def test_device_initialisers(gpu_lib, kind, bcs):
+    """The reference's built-in initialisers run on the device, then the ghost
+    fill, against the reference's own initialise + apply_boundary +
+    primitiveToConserved (main.cpp:85-99): every cell, ghosts included.
+    Bit for bit, except sine_x, whose sin() may differ in the last bit between
+    CUDA and the host C library (relative 1e-15)."""
+    n = (12, 10, 6)
+    P, G = make_params(n=n, L=(1.0, 1.0, 0.5), bcs=bcs)
+    ref = oracle.RefSolver(P, G)
+    ref.initialize(kind)
+    with solver(P, G) as s:
+        s.initialize(kind)
+        W = s.primitives()
+        U = s.conserved()
+    Wr = np.stack([ref.get(k) for k in ("rho", "u", "v", "w", "p")])
+    Ur = ref.conserved()
+    if kind == "sine_x":
+        assert per_var(W, Wr) <= 1e-15 and per_var(U, Ur) <= 1e-15
+    else:
+        assert np.array_equal(W, Wr) and np.array_equal(U, Ur)
+    # and the state then steps like the reference's
+    ref.rk3_step(1e-4)
+    with solver(P, G) as s:
+        s.initialize(kind)
+        s.rk3_step(1e-4)
+        assert per_var(s.conserved(), ref.conserved()) <= STEP_TOL

@@ -52,6 +52,53 @@ def test_noalloc_timestep_matches_handle_entry_point(gpu_lib, n, seed):
     assert results[0] == results[1]
 
 
+def _handle_dt_and_fields(n, P, G, st):
+    import torch
+    from ns3d_wcns_b200.solver import Solver
+    with Solver(P, G) as s:
+        s.set_interior_primitives(*st)
+        expected = s.compute_timestep()
+        W = s.primitives()
+    return expected, [torch.from_numpy(np.ascontiguousarray(W[q])).cuda() for q in range(5)]
+
+
+def test_noalloc_multi_block_then_smaller_grid(gpu_lib):
+    """64 x 48 x 40 needs 15 blocks of partials, so the combine reads several;
+    a following call on a smaller grid whose minimum is larger writes fewer
+    partials than the first call left behind, and must still return its own
+    grid's time step (only the partials a call writes are read)."""
+    import torch
+    lib = _lib.load()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    big = (64, 48, 40)
+    Pb, Gb = make_params(n=big, L=(2 * np.pi, 1.5 * np.pi, 1.25 * np.pi), Ma=0.3, cfl=0.5, dt_fixed=-1.0)
+    st_big = random_state(big, seed=7, amp=0.3)
+    small = (20, 12, 10)
+    Ps, Gs = make_params(n=small, L=(2 * np.pi, 1.2 * np.pi, np.pi), Ma=0.3, cfl=0.5, dt_fixed=-1.0)
+    st_small = random_state(small, seed=8, amp=0.05)
+    # the small grid is coarser and its state slower (smaller |u| + a), so
+    # its time step is larger than the big grid's: a leftover big-grid
+    # partial would show
+    st_small = [st_small[0], st_small[1] * 0.2, st_small[2] * 0.2, st_small[3] * 0.2, st_small[4]]
+    exp_big, f_big = _handle_dt_and_fields(big, Pb, Gb, st_big)
+    exp_small, f_small = _handle_dt_and_fields(small, Ps, Gs, st_small)
+    assert exp_small > exp_big  # every big-grid partial is below the small grid's minimum
+    out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    assert _call(lib, f_big, big, Pb, Gb, out, stream) == 0
+    torch.cuda.synchronize()
+    assert abs(float(out.item()) - exp_big) <= 1e-14 * exp_big
+    out.fill_(-1.0)
+    assert _call(lib, f_small, small, Ps, Gs, out, stream) == 0
+    torch.cuda.synchronize()
+    assert abs(float(out.item()) - exp_small) <= 1e-14 * exp_small
+    # and the big grid once more, after the small one
+    out.fill_(-1.0)
+    assert _call(lib, f_big, big, Pb, Gb, out, stream) == 0
+    torch.cuda.synchronize()
+    assert abs(float(out.item()) - exp_big) <= 1e-14 * exp_big
+
+
 def test_noalloc_rejects_grids_beyond_its_scratch(gpu_lib):
     import torch
     lib = _lib.load()
