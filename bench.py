@@ -180,17 +180,21 @@ def run_reference(args, rank):
 
 # --------------------------------------------------------------- adjoint
 
-def adjoint_report(device: int, n: int = 64, nsteps: int = 200, dt: float = 2e-3, ce: int = 20, ndir: int = 16):
+def adjoint_report(device: int, n: int = 64, nsteps: int = 200, dt: float = 2e-3, ce: int = 20, ndir: int = 16,
+                   interp: int = 0, riemann: int = 0):
     """Config 4: 64^3 isotropic, Re 200, dt 2e-3, 200 RK3 steps, checkpoint every 20;
     gradient of the final kinetic energy w.r.t. the initial velocity, checked
-    against central finite differences (h = 1e-6) on ndir seeded directions."""
+    against central finite differences (h = 1e-6) on ndir seeded directions.
+    interp / riemann: WENO5 + Roe (0, 0) or the benchmark scheme MDCD_HYBRID +
+    HLLC (3, 2), whose detector is a switch: FD differences that straddle a
+    switching face are not derivatives, which the h / 2h comparison shows."""
     import numpy as np
     import math
     from ns3d_wcns_b200.config import make_params
     from ns3d_wcns_b200.initial import isotropic_state
     from ns3d_wcns_b200.solver import Solver
     P, G = make_params(n=(n, n, n), L=(2 * math.pi,) * 3, Ma=0.3, Re=200.0, Pr=0.72, dt_fixed=dt,
-                       interpolation=0, riemann=0, S_ref=110.4 / 273.15)
+                       interpolation=interp, riemann=riemann, S_ref=110.4 / 273.15)
     st = isotropic_state((n, n, n), P.gamma, P.Ma, seed=4)
     rng = np.random.default_rng(16)
     with Solver(P, G, device=device) as s:
@@ -234,7 +238,8 @@ def adjoint_report(device: int, n: int = 64, nsteps: int = 200, dt: float = 2e-3
             errs4.append(abs(fd4 - ad) / abs(fd4))
             errsn.append(abs(fd - ad) / (gnorm * float(np.sqrt(np.sum(d * d)))))
             noise.append(abs(fd - fd2) / abs(fd))   # size of the FD's own error
-    return {"config": f"{n}^3 isotropic WENO5+Roe, Re 200, dt {dt}, {nsteps} steps, checkpoint every {ce}",
+    scheme = {(0, 0): "WENO5+Roe", (3, 2): "MDCD_HYBRID+HLLC", (2, 2): "MDCD_LINEAR+HLLC"}.get((interp, riemann))
+    return {"config": f"{n}^3 isotropic {scheme}, Re 200, dt {dt}, {nsteps} steps, checkpoint every {ce}",
             "J": J2, "forward_ms": stats2["forward_ms"], "adjoint_ms": stats2["adjoint_ms"],
             "adjoint_over_forward": stats2["adjoint_ms"] / stats2["forward_ms"],
             "plain_forward_ms": plain_forward_ms,
@@ -820,9 +825,10 @@ def main():
         g512 = {**res, "mixed_over_fp64": res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"],
                 "unit": "cell-updates/s", "steps": args.steps}
 
-    adjoint = None
+    adjoint = adjoint_hyb = None
     if not args.no_adjoint and rank == 0:
         adjoint = adjoint_report(local)
+        adjoint_hyb = adjoint_report(local, interp=3, riemann=2)
     batched = None
     if not args.no_batch and rank == 0:
         batched = batched_report(local, args.batch_problems)
@@ -844,7 +850,7 @@ def main():
                                  "captured device time loop, which event profiling cannot enter)",
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "kinetic_energy_end": ke64,
-            "adjoint": adjoint,
+            "adjoint": adjoint, "adjoint_benchmark_scheme": adjoint_hyb,
             "batched": batched,
         }
         print(json.dumps(line), flush=True)

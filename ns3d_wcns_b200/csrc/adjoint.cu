@@ -93,24 +93,14 @@ __global__ void __launch_bounds__(ADJ_T) adj_face_kernel(AdjArgs a) {
 #pragma unroll
         for (int m = 0; m < 6; ++m) f[m] = sSt[q * 6 + m][tid];
         double l, r;
-        if constexpr (INTERP == 0) {
-            const double fr[5] = {f[5], f[4], f[3], f[2], f[1]};
-            l = adj::weno5_fwd(f);
-            r = adj::weno5_fwd(fr);
-        } else {
-            l = 0.0; r = 0.0;
-#pragma unroll
-            for (int m = 0; m < 6; ++m) { l += a.lin[m] * f[m]; r += a.lin[m] * f[5 - m]; }
-        }
+        adj::interp_pair_fwd<double, INTERP>(f, a.lin, a.hd, l, r);
         sLR[q][tid] = l;
         sLR[5 + q][tid] = r;
     }
     double UL[5], UR[5], ULb[5] = {0, 0, 0, 0, 0}, URb[5] = {0, 0, 0, 0, 0};
 #pragma unroll
     for (int q = 0; q < 5; ++q) { UL[q] = sLR[q][tid]; UR[q] = sLR[5 + q][tid]; }
-    if constexpr (RS == 0) adj::roe_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
-    else if constexpr (RS == 1) adj::rusanov_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
-    else adj::hll_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
+    adj::riemann_vjp<DIR, double, RS>(UL, UR, a.gamma, Fb, ULb, URb);
 #pragma unroll
     for (int q = 0; q < 5; ++q) { sLR[q][tid] = ULb[q]; sLR[5 + q][tid] = URb[q]; }
     // interpolation VJP, one variable at a time, straight into the face store
@@ -120,18 +110,7 @@ __global__ void __launch_bounds__(ADJ_T) adj_face_kernel(AdjArgs a) {
 #pragma unroll
         for (int m = 0; m < 6; ++m) f[m] = sSt[q * 6 + m][tid];
         const double lb = sLR[q][tid], rb = sLR[5 + q][tid];
-        if constexpr (INTERP == 0) {
-            double fbl[5] = {0, 0, 0, 0, 0}, fbr[5] = {0, 0, 0, 0, 0};
-            adj::weno5_vjp(f, lb, fbl);
-            const double fr[5] = {f[5], f[4], f[3], f[2], f[1]};
-            adj::weno5_vjp(fr, rb, fbr);
-            gb[0] = fbl[0]; gb[5] = fbr[0];
-#pragma unroll
-            for (int m = 1; m < 5; ++m) gb[m] = fbl[m] + fbr[5 - m];
-        } else {
-#pragma unroll
-            for (int m = 0; m < 6; ++m) gb[m] = a.lin[m] * lb + a.lin[5 - m] * rb;
-        }
+        adj::interp_pair_vjp<double, INTERP>(f, a.lin, a.hd, lb, rb, gb);
 #pragma unroll
         for (int m = 0; m < 6; ++m) a.G[m * 5 + q][t] = gb[m];
     }
@@ -185,24 +164,14 @@ __global__ void __launch_bounds__(256) adj_line_kernel(AdjArgs a, int lpb, int f
 #pragma unroll
             for (int m = 0; m < 6; ++m) f[m] = sU[q * T + at(c - 2 + m)];
             double lv, rv;
-            if constexpr (INTERP == 0) {
-                const double fr[5] = {f[5], f[4], f[3], f[2], f[1]};
-                lv = adj::weno5_fwd(f);
-                rv = adj::weno5_fwd(fr);
-            } else {
-                lv = 0.0; rv = 0.0;
-#pragma unroll
-                for (int m = 0; m < 6; ++m) { lv += a.lin[m] * f[m]; rv += a.lin[m] * f[5 - m]; }
-            }
+            adj::interp_pair_fwd<double, INTERP>(f, a.lin, a.hd, lv, rv);
             sLR[q * T + tid] = lv;
             sLR[(5 + q) * T + tid] = rv;
         }
         double UL[5], UR[5], ULb[5] = {0, 0, 0, 0, 0}, URb[5] = {0, 0, 0, 0, 0};
 #pragma unroll
         for (int q = 0; q < 5; ++q) { UL[q] = sLR[q * T + tid]; UR[q] = sLR[(5 + q) * T + tid]; }
-        if constexpr (RS == 0) adj::roe_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
-        else if constexpr (RS == 1) adj::rusanov_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
-        else adj::hll_vjp<DIR, double>(UL, UR, a.gamma, Fb, ULb, URb);
+        adj::riemann_vjp<DIR, double, RS>(UL, UR, a.gamma, Fb, ULb, URb);
 #pragma unroll
         for (int q = 0; q < 5; ++q) { sLR[q * T + tid] = ULb[q]; sLR[(5 + q) * T + tid] = URb[q]; }
 #pragma unroll 1
@@ -211,18 +180,7 @@ __global__ void __launch_bounds__(256) adj_line_kernel(AdjArgs a, int lpb, int f
 #pragma unroll
             for (int m = 0; m < 6; ++m) f[m] = sU[q * T + at(c - 2 + m)];
             const double lb = sLR[q * T + tid], rb = sLR[(5 + q) * T + tid];
-            if constexpr (INTERP == 0) {
-                double fbl[5] = {0, 0, 0, 0, 0}, fbr[5] = {0, 0, 0, 0, 0};
-                adj::weno5_vjp(f, lb, fbl);
-                const double fr[5] = {f[5], f[4], f[3], f[2], f[1]};
-                adj::weno5_vjp(fr, rb, fbr);
-                gb[0] = fbl[0]; gb[5] = fbr[0];
-#pragma unroll
-                for (int m = 1; m < 5; ++m) gb[m] = fbl[m] + fbr[5 - m];
-            } else {
-#pragma unroll
-                for (int m = 0; m < 6; ++m) gb[m] = a.lin[m] * lb + a.lin[5 - m] * rb;
-            }
+            adj::interp_pair_vjp<double, INTERP>(f, a.lin, a.hd, lb, rb, gb);
 #pragma unroll
             for (int m = 0; m < 6; ++m) sG[(m * 5 + q) * T + tid] = gb[m];
         }
@@ -434,30 +392,33 @@ __global__ void step_combine_kernel(int which, double *const *tab, double dt, lo
 cudaError_t adj_rhs_vjp(const AdjArgs &a, cudaStream_t st, long *launches) {
     const long n = (long)a.L.nx * a.L.ny * a.L.nz;
     const int nb = blocks_for(n, 128);
-    // riemann codes here: 0 Roe, 1 Rusanov, 3 HLL (face_vjp_t takes 2 for HLL)
-    const int rs = a.riemann == 3 ? 2 : a.riemann;
+    // riemann_vjp codes: 0 Roe, 1 Rusanov, 2 HLL, 3 HLLC (from the public value)
+    const int rs = adj::adj_riemann_code(a.riemann);
     auto face = [&](auto dir_tag) {
         constexpr int D = decltype(dir_tag)::value;
-        if (a.interp == 0) {
-            if (rs == 0) adj_face_kernel<D, 0, 0><<<nb, 128, 0, st>>>(a);
-            else if (rs == 1) adj_face_kernel<D, 0, 1><<<nb, 128, 0, st>>>(a);
-            else adj_face_kernel<D, 0, 2><<<nb, 128, 0, st>>>(a);
-        } else {
-            if (rs == 0) adj_face_kernel<D, 2, 0><<<nb, 128, 0, st>>>(a);
-            else if (rs == 1) adj_face_kernel<D, 2, 1><<<nb, 128, 0, st>>>(a);
-            else adj_face_kernel<D, 2, 2><<<nb, 128, 0, st>>>(a);
-        }
+        auto go = [&](auto it) {
+            constexpr int I = decltype(it)::value;
+            if (rs == 0) adj_face_kernel<D, I, 0><<<nb, 128, 0, st>>>(a);
+            else if (rs == 1) adj_face_kernel<D, I, 1><<<nb, 128, 0, st>>>(a);
+            else if (rs == 2) adj_face_kernel<D, I, 2><<<nb, 128, 0, st>>>(a);
+            else adj_face_kernel<D, I, 3><<<nb, 128, 0, st>>>(a);
+        };
+        if (a.interp == 0) go(std::integral_constant<int, 0>{});
+        else if (a.interp == 2) go(std::integral_constant<int, 2>{});
+        else go(std::integral_constant<int, 3>{});
     };
     auto line = [&](auto dir_tag, int first) -> cudaError_t {
         constexpr int D = decltype(dir_tag)::value;
-        if (a.interp == 0) {
-            if (rs == 0) return launch_line<D, 0, 0>(a, first, st);
-            if (rs == 1) return launch_line<D, 0, 1>(a, first, st);
-            return launch_line<D, 0, 2>(a, first, st);
-        }
-        if (rs == 0) return launch_line<D, 2, 0>(a, first, st);
-        if (rs == 1) return launch_line<D, 2, 1>(a, first, st);
-        return launch_line<D, 2, 2>(a, first, st);
+        auto go = [&](auto it) -> cudaError_t {
+            constexpr int I = decltype(it)::value;
+            if (rs == 0) return launch_line<D, I, 0>(a, first, st);
+            if (rs == 1) return launch_line<D, I, 1>(a, first, st);
+            if (rs == 2) return launch_line<D, I, 2>(a, first, st);
+            return launch_line<D, I, 3>(a, first, st);
+        };
+        if (a.interp == 0) return go(std::integral_constant<int, 0>{});
+        if (a.interp == 2) return go(std::integral_constant<int, 2>{});
+        return go(std::integral_constant<int, 3>{});
     };
     const bool fused = a.L.nx <= 256 && a.L.ny <= 256 && a.L.nz <= 256;
     if (fused) {
@@ -521,23 +482,26 @@ extern "C" int ns3d_debug_face_vjp(int direction, int interpolation, int riemann
                                    double *flux5) {
     using namespace ns3d;
     if (!U30 || !Fbar5 || !out30 || direction < 0 || direction > 2) return -1;
-    if (interpolation != 0 && interpolation != 2) return -2;
-    if (riemann < 0 || riemann > 3 || riemann == 2) return -2;
+    if (interpolation != 0 && interpolation != 2 && interpolation != 3) return -2;
+    if (interpolation != 0 && !lin) return -1;
+    const int rs = adj::adj_riemann_code(riemann);
+    if (rs < 0) return -2;
     double U[5][6], Ub[5][6] = {};
     for (int q = 0; q < 5; ++q)
         for (int m = 0; m < 6; ++m) U[q][m] = U30[q * 6 + m];
-    const int rs = riemann == 3 ? 2 : riemann;  // 0 Roe, 1 Rusanov, 3 HLL
-    if (direction == 0) adj::face_vjp<0, double>(interpolation, rs, lin, gamma, U, Fbar5, Ub);
-    else if (direction == 1) adj::face_vjp<1, double>(interpolation, rs, lin, gamma, U, Fbar5, Ub);
-    else adj::face_vjp<2, double>(interpolation, rs, lin, gamma, U, Fbar5, Ub);
+    const double zero6[6] = {0, 0, 0, 0, 0, 0};
+    const double *li = lin ? lin : zero6, *hd = interpolation == 3 ? lin + 6 : zero6;
+    if (direction == 0) adj::face_vjp<0, double>(interpolation, rs, li, hd, gamma, U, Fbar5, Ub);
+    else if (direction == 1) adj::face_vjp<1, double>(interpolation, rs, li, hd, gamma, U, Fbar5, Ub);
+    else adj::face_vjp<2, double>(interpolation, rs, li, hd, gamma, U, Fbar5, Ub);
     for (int q = 0; q < 5; ++q)
         for (int m = 0; m < 6; ++m) out30[q * 6 + m] = Ub[q][m];
     if (flux5) {
         // forward face flux with the production functions (schemes.cuh)
         SchemeParams<double> sp;
         sp.gamma = gamma;
-        for (int m = 0; m < 6; ++m) sp.lin[m] = lin ? lin[m] : 0.0;
-        for (int m = 0; m < 4; ++m) sp.hd[m] = 0.0;
+        for (int m = 0; m < 6; ++m) sp.lin[m] = li[m];
+        for (int m = 0; m < 4; ++m) sp.hd[m] = interpolation == 3 ? hd[m] : 0.0;
         sp.interp = interpolation; sp.riemann = riemann; sp.char_recon = 0;
         double wi[5] = {0, 0, 0, 0, 0};
         if (direction == 0) wcns_face<0, double, RUNTIME, RUNTIME, 0>(sp, U, wi, wi, flux5);

@@ -8,14 +8,17 @@
 // differences on the host (tests/test_adjoint_cpu.py through
 // ns3d_debug_face_vjp) and runs in the adjoint kernels.
 //
-// Supported: WENO5 and MDCD_LINEAR component-wise interpolation; Roe,
-// Rusanov and HLL fluxes.  The state differentiated is the conserved U (the
+// Supported: WENO5, MDCD_LINEAR and MDCD_HYBRID component-wise
+// interpolation; Roe, Rusanov, HLL and HLLC fluxes.  MDCD_HYBRID's detector
+// is a switch: its derivative is zero, and the active branch (linear or
+// WENO) is differentiated.  The state differentiated is the conserved U (the
 // c2p/p2c round trip of runge_kutta_3 is the identity mathematically).
 #pragma once
 
 #include <math.h>
 
 #include "common.cuh"
+#include "schemes.cuh"
 
 #ifndef NS3D_HD
 #define NS3D_HD __host__ __device__ __forceinline__
@@ -79,6 +82,129 @@ NS3D_HD void weno5_vjp(const R *f, R qb, R *fb) {
     fb[1] += tb + ub; fb[2] += R(-2) * tb; fb[3] += tb - ub;
     tb = R(2) * c13 * t2 * bb2; ub = R(0.5) * u2 * bb2;
     fb[2] += tb + R(3) * ub; fb[3] += R(-2) * tb - R(4) * ub; fb[4] += tb + ub;
+}
+
+// MDCD_HYBRID's WENO branch (mdcd_weno_branch, interpolation.cpp:170-208)
+// VJP: q = sum al_k q_k / (8 sum al_k), al_k = d_k (20 + tau6/(beta_k + 1e-40))^2,
+// tau6 = |beta3 - (beta0 + 4 beta1 + beta2)/6|; fb[0..5] += dq/df * qb.
+template <typename R>
+NS3D_HD void mdcd_weno_vjp(const R *f, const R *hd, R qb, R *fb) {
+    const R c13 = R(13.0 / 12.0), es = R(1e-40);
+    const R t0 = f[0] - R(2) * f[1] + f[2], u0 = f[0] - R(4) * f[1] + R(3) * f[2];
+    const R t1 = f[1] - R(2) * f[2] + f[3], u1 = f[1] - f[3];
+    const R t2 = f[2] - R(2) * f[3] + f[4], u2 = R(3) * f[2] - R(4) * f[3] + f[4];
+    const R be[4] = {c13 * (t0 * t0) + R(0.25) * (u0 * u0), c13 * (t1 * t1) + R(0.25) * (u1 * u1),
+                     c13 * (t2 * t2) + R(0.25) * (u2 * u2), mdcd_beta3(f[0], f[1], f[2], f[3], f[4], f[5])};
+    const R qk[4] = {R(3) * f[0] - R(10) * f[1] + R(15) * f[2], -f[1] + R(6) * f[2] + R(3) * f[3],
+                     R(3) * f[2] + R(6) * f[3] - f[4], R(15) * f[3] - R(10) * f[4] + R(3) * f[5]};
+    const R D = be[3] - (be[0] + R(4) * be[1] + be[2]) / R(6);
+    const R tau = fabs(D);
+    R g[4], al[4], A = R(0), Q = R(0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        g[k] = R(20) + tau / (be[k] + es);
+        al[k] = hd[k] * (g[k] * g[k]);
+        A += al[k];
+        Q += al[k] * qk[k];
+    }
+    const R q = Q / (R(8) * A);
+    R qkb[4], beb[4], taub = R(0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        qkb[k] = qb * al[k] / (R(8) * A);
+        const R alb = qb * (qk[k] * R(0.125) - q) / A;
+        const R gb = alb * R(2) * hd[k] * g[k];
+        const R ib = R(1) / (be[k] + es);
+        taub += gb * ib;
+        beb[k] = -gb * tau * ib * ib;
+    }
+    const R Db = D >= R(0) ? taub : -taub;
+    beb[3] += Db;
+    beb[0] -= Db / R(6);
+    beb[1] -= R(4) * Db / R(6);
+    beb[2] -= Db / R(6);
+    // candidates
+    fb[0] += R(3) * qkb[0];
+    fb[1] += R(-10) * qkb[0] - qkb[1];
+    fb[2] += R(15) * qkb[0] + R(6) * qkb[1] + R(3) * qkb[2];
+    fb[3] += R(3) * qkb[1] + R(6) * qkb[2] + R(15) * qkb[3];
+    fb[4] += -qkb[2] - R(10) * qkb[3];
+    fb[5] += R(3) * qkb[3];
+    // beta0..beta2
+    R tb = R(2) * c13 * t0 * beb[0], ub = R(0.5) * u0 * beb[0];
+    fb[0] += tb + ub; fb[1] += R(-2) * tb - R(4) * ub; fb[2] += tb + R(3) * ub;
+    tb = R(2) * c13 * t1 * beb[1]; ub = R(0.5) * u1 * beb[1];
+    fb[1] += tb + ub; fb[2] += R(-2) * tb; fb[3] += tb - ub;
+    tb = R(2) * c13 * t2 * beb[2]; ub = R(0.5) * u2 * beb[2];
+    fb[2] += tb + R(3) * ub; fb[3] += R(-2) * tb - R(4) * ub; fb[4] += tb + ub;
+    // beta3: gradient of the quadratic form of interpolation.cpp:193-200
+    const R b3 = beb[3] / R(120960);
+    fb[0] += b3 * (R(543598) * f[0] - R(2380800) * f[1] + R(4086352) * f[2] - R(3462252) * f[3] +
+                   R(1458762) * f[4] - R(245620) * f[5]);
+    fb[1] += b3 * (R(-2380800) * f[0] + R(11306634) * f[1] - R(20427884) * f[2] + R(17905032) * f[3] -
+                   R(7727988) * f[4] + R(1325006) * f[5]);
+    fb[2] += b3 * (R(4086352) * f[0] - R(20427884) * f[1] + R(39021944) * f[2] - R(35817664) * f[3] +
+                   R(15929912) * f[4] - R(2792660) * f[5]);
+    fb[3] += b3 * (R(-3462252) * f[0] + R(17905032) * f[1] - R(35817664) * f[2] + R(34391304) * f[3] -
+                   R(15880404) * f[4] + R(2863984) * f[5]);
+    fb[4] += b3 * (R(1458762) * f[0] - R(7727988) * f[1] + R(15929912) * f[2] - R(15880404) * f[3] +
+                   R(7649694) * f[4] - R(1429976) * f[5]);
+    fb[5] += b3 * (R(-245620) * f[0] + R(1325006) * f[1] - R(2792660) * f[2] + R(2863984) * f[3] -
+                   R(1429976) * f[4] + R(279266) * f[5]);
+}
+
+// Left and right interpolated states of one variable at a face from its
+// stencil f[0..5] (cells i-2 .. i+3) -- INTERP 0 WENO5, 2 MDCD_LINEAR,
+// 3 MDCD_HYBRID (the decision of both sides is the detector at cells i and
+// i+1, as in the sweeps) -- and their VJP into gb[0..5].
+template <typename R, int INTERP>
+NS3D_HD void interp_pair_fwd(const R *f, const R *lin, const R *hd, R &l, R &r) {
+    const R fr[6] = {f[5], f[4], f[3], f[2], f[1], f[0]};
+    if constexpr (INTERP == 0) {
+        l = weno5_fwd(f);
+        r = weno5_fwd(fr);
+        return;
+    }
+    if constexpr (INTERP == 3) {
+        if (!(mdcd_smooth(f[0], f[1], f[2], f[3], f[4]) && mdcd_smooth(f[1], f[2], f[3], f[4], f[5]))) {
+            l = mdcd_weno_branch(hd, f[0], f[1], f[2], f[3], f[4], f[5]);
+            r = mdcd_weno_branch(hd, fr[0], fr[1], fr[2], fr[3], fr[4], fr[5]);
+            return;
+        }
+    }
+    l = R(0);
+    r = R(0);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) { l += lin[m] * f[m]; r += lin[m] * fr[m]; }
+}
+
+template <typename R, int INTERP>
+NS3D_HD void interp_pair_vjp(const R *f, const R *lin, const R *hd, R lb, R rb, R *gb) {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) gb[m] = R(0);
+    if constexpr (INTERP == 0) {
+        R fbl[5] = {0, 0, 0, 0, 0}, fbr[5] = {0, 0, 0, 0, 0};
+        weno5_vjp(f, lb, fbl);
+        const R fr[5] = {f[5], f[4], f[3], f[2], f[1]};
+        weno5_vjp(fr, rb, fbr);
+        gb[0] = fbl[0]; gb[5] = fbr[0];
+#pragma unroll
+        for (int m = 1; m < 5; ++m) gb[m] = fbl[m] + fbr[5 - m];
+        return;
+    }
+    if constexpr (INTERP == 3) {
+        if (!(mdcd_smooth(f[0], f[1], f[2], f[3], f[4]) && mdcd_smooth(f[1], f[2], f[3], f[4], f[5]))) {
+            R fbr[6] = {0, 0, 0, 0, 0, 0};
+            const R fr[6] = {f[5], f[4], f[3], f[2], f[1], f[0]};
+            mdcd_weno_vjp(f, hd, lb, gb);
+            mdcd_weno_vjp(fr, hd, rb, fbr);
+#pragma unroll
+            for (int m = 0; m < 6; ++m) gb[m] += fbr[5 - m];
+            return;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) gb[m] = lin[m] * lb + lin[5 - m] * rb;
 }
 
 // ------------------------------------------------------------ Riemann VJPs
@@ -354,63 +480,181 @@ NS3D_HD void hll_vjp(const R *UL, const R *UR, R g, const R *Fb, R *ULb, R *URb)
     side_vjp(Rs, g, uRb, vRb, wRb, pRb, ERb, rRb, URb);
 }
 
+// HLLC flux (HLLC_Riemann_solver, InviscousFlux.cpp:449-592, as hllc_flux of
+// schemes.cuh evaluates it) VJP: Davis wave speeds S_L = min(un_L - a_L,
+// un_R - a_R), S_R = max(un_L + a_L, un_R + a_R) (the active arm
+// differentiated), the Batten contact speed S_M (or its Roe-average
+// fallback) and the upwind side's star state.
+template <int DIR, typename R>
+NS3D_HD void hllc_vjp(const R *UL, const R *UR, R g, const R *Fb, R *ULb, R *URb) {
+    SideF<R> L = side_fwd(UL, g), Rs = side_fwd(UR, g);
+    const R unL = DIR == 0 ? L.u : (DIR == 1 ? L.v : L.w), unR = DIR == 0 ? Rs.u : (DIR == 1 ? Rs.v : Rs.w);
+    const R aL = sqrt(g * L.p * L.ir), aR = sqrt(g * Rs.p * Rs.ir);
+    R a = unL - aL, b = unR - aR;
+    const bool sl_right = b < a;
+    const R SL = sl_right ? b : a;
+    a = unL + aL; b = unR + aR;
+    const bool sr_right = a < b;
+    const R SR = sr_right ? b : a;
+    R uLb = 0, vLb = 0, wLb = 0, pLb = 0, ELb = 0, rLb = 0, irLb = 0;
+    R uRb = 0, vRb = 0, wRb = 0, pRb = 0, ERb = 0, rRb = 0, irRb = 0;
+    if (SL >= R(0) || SR <= R(0)) {
+        const bool left = SL >= R(0);
+        if (left) pflux_vjp<DIR, R>(L, Fb, uLb, vLb, wLb, pLb, ELb, rLb);
+        else pflux_vjp<DIR, R>(Rs, Fb, uRb, vRb, wRb, pRb, ERb, rRb);
+        side_vjp(L, g, uLb, vLb, wLb, pLb, ELb, rLb, ULb);
+        side_vjp(Rs, g, uRb, vRb, wRb, pRb, ERb, rRb, URb);
+        return;
+    }
+    const R num = Rs.r * unR * (SR - unR) - L.r * unL * (SL - unL) + L.p - Rs.p;
+    const R den = Rs.r * (SR - unR) - L.r * (SL - unL);
+    const bool batten = fabs(den) > R(1e-12);
+    R SM;
+    const R sqL = sqrt(L.r), sqR = sqrt(Rs.r);
+    if (batten) SM = num / den;
+    else SM = (sqL * unL + sqR * unR) / (sqL + sqR);
+    // the upwind side K and its star state
+    const bool left = SM >= R(0);
+    const SideF<R> &K = left ? L : Rs;
+    const R *UK = left ? UL : UR;
+    R *UKb = left ? ULb : URb;
+    const R unK = left ? unL : unR, Sk = left ? SL : SR;
+    const R dk = Sk - unK, W = Sk - SM, P = K.r * dk;
+    const R rs = K.r * dk / W;
+    const R Z = K.p / P, X = SM - unK, Y = SM + Z;
+    const R Es = K.E * K.ir + X * Y;
+    const R vs[5] = {R(1), DIR == 0 ? SM : K.u, DIR == 1 ? SM : K.v, DIR == 2 ? SM : K.w, Es};
+    // F_n = FK_n + Sk (rs vs_n - UK_n)
+    R Skb = R(0), rsb = R(0), vsb[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+        Skb += Fb[n] * (rs * vs[n] - UK[n]);
+        rsb += Sk * Fb[n] * vs[n];
+        vsb[n] = Sk * rs * Fb[n];
+        UKb[n] -= Sk * Fb[n];
+    }
+    R uKb = 0, vKb = 0, wKb = 0, pKb = 0, EKb = 0, rKb = 0, irKb = 0, unKb = 0, SMb = 0, dkb = 0;
+    if (DIR == 0) SMb += vsb[1]; else uKb += vsb[1];
+    if (DIR == 1) SMb += vsb[2]; else vKb += vsb[2];
+    if (DIR == 2) SMb += vsb[3]; else wKb += vsb[3];
+    // Es = E ir + X Y, X = SM - un, Y = SM + p / (r dk)
+    const R Esb = vsb[4];
+    EKb += Esb * K.ir;
+    irKb += Esb * K.E;
+    const R Xb = Esb * Y, Yb = Esb * X;
+    SMb += Xb + Yb;
+    unKb -= Xb;
+    pKb += Yb / P;
+    const R Pb = -Yb * K.p / (P * P);
+    rKb += Pb * dk;
+    dkb += Pb * K.r;
+    // rs = r dk / (Sk - SM)
+    rKb += rsb * dk / W;
+    dkb += rsb * K.r / W;
+    const R Wb = -rsb * K.r * dk / (W * W);
+    Skb += Wb;
+    SMb -= Wb;
+    // dk = Sk - un
+    Skb += dkb;
+    unKb -= dkb;
+    // the physical flux of side K
+    pflux_vjp<DIR, R>(K, Fb, uKb, vKb, wKb, pKb, EKb, rKb);
+    if (DIR == 0) uKb += unKb; else if (DIR == 1) vKb += unKb; else wKb += unKb;
+    if (left) {
+        uLb += uKb; vLb += vKb; wLb += wKb; pLb += pKb; ELb += EKb; rLb += rKb; irLb += irKb;
+    } else {
+        uRb += uKb; vRb += vKb; wRb += wKb; pRb += pKb; ERb += EKb; rRb += rKb; irRb += irKb;
+    }
+    R SLb = left ? Skb : R(0), SRb = left ? R(0) : Skb;
+    R unLb = 0, unRb = 0;
+    if (batten) {
+        const R numb = SMb / den, denb = -SMb * SM / den;
+        rRb += numb * unR * (SR - unR) + denb * (SR - unR);
+        unRb += numb * Rs.r * (SR - R(2) * unR) - denb * Rs.r;
+        SRb += numb * Rs.r * unR + denb * Rs.r;
+        rLb -= numb * unL * (SL - unL) + denb * (SL - unL);
+        unLb -= numb * L.r * (SL - R(2) * unL) - denb * L.r;
+        SLb -= numb * L.r * unL + denb * L.r;
+        pLb += numb;
+        pRb -= numb;
+    } else {
+        const R S = sqL + sqR, N = sqL * unL + sqR * unR;
+        const R Nb = SMb / S, Sb = -SMb * N / (S * S);
+        unLb += Nb * sqL;
+        unRb += Nb * sqR;
+        rLb += (Nb * unL + Sb) / (R(2) * sqL);
+        rRb += (Nb * unR + Sb) / (R(2) * sqR);
+    }
+    // wave speeds: S_L = un - a of the minimising side, S_R = un + a of the maximising side
+    R aLb = 0, aRb = 0;
+    if (sl_right) { unRb += SLb; aRb -= SLb; } else { unLb += SLb; aLb -= SLb; }
+    if (sr_right) { unRb += SRb; aRb += SRb; } else { unLb += SRb; aLb += SRb; }
+    // a = sqrt(g p ir)
+    if (aL > R(0)) { const R xb = aLb / (R(2) * aL); pLb += xb * g * L.ir; irLb += xb * g * L.p; }
+    if (aR > R(0)) { const R xb = aRb / (R(2) * aR); pRb += xb * g * Rs.ir; irRb += xb * g * Rs.p; }
+    if (DIR == 0) { uLb += unLb; uRb += unRb; }
+    else if (DIR == 1) { vLb += unLb; vRb += unRb; }
+    else { wLb += unLb; wRb += unRb; }
+    // ir = 1 / r
+    rLb -= irLb * L.ir * L.ir;
+    rRb -= irRb * Rs.ir * Rs.ir;
+    side_vjp(L, g, uLb, vLb, wLb, pLb, ELb, rLb, ULb);
+    side_vjp(Rs, g, uRb, vRb, wRb, pRb, ERb, rRb, URb);
+}
+
+// Riemann VJP by code: 0 Roe, 1 Rusanov, 2 HLL, 3 HLLC.
+template <int DIR, typename R, int RS>
+NS3D_HD void riemann_vjp(const R *UL, const R *UR, R g, const R *Fb, R *ULb, R *URb) {
+    if constexpr (RS == 0) roe_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
+    else if constexpr (RS == 1) rusanov_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
+    else if constexpr (RS == 2) hll_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
+    else hllc_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
+}
+
+// VJP code of a public riemann_solver value (NS3D_ROE 0, NS3D_RUSANOV 1,
+// NS3D_HLLC 2, NS3D_HLL 3), -1 when it has no VJP.
+NS3D_HD int adj_riemann_code(int rs) {
+    return rs == 0 ? 0 : rs == 1 ? 1 : rs == 3 ? 2 : rs == 2 ? 3 : -1;
+}
+
 // ------------------------------------------------------------ face VJP
 
 // Component-wise WCNS face flux (WCNS_Riemann_InviscidFlux, InviscousFlux.cpp:
 // 146-268 with char_recon = false): U[n][m], m = cells i-2..i+3.
-// interp: 0 WENO5, 2 MDCD_LINEAR (lin = its six coefficients).
+// INTERP: 0 WENO5, 2 MDCD_LINEAR (lin = its six coefficients), 3 MDCD_HYBRID
+// (also hd = its WENO weights d0..d3); RS: a riemann_vjp code.
 template <int DIR, typename R, int INTERP, int RS>
-NS3D_HD void face_vjp_t(const R *lin, R g, const R U[5][6], const R *Fb, R Ub[5][6]) {
-    constexpr int interp = INTERP, riemann = RS;
+NS3D_HD void face_vjp_t(const R *lin, const R *hd, R g, const R U[5][6], const R *Fb, R Ub[5][6]) {
     R UL[5], UR[5];
 #pragma unroll
-    for (int n = 0; n < 5; ++n) {
-        const R *f = U[n];
-        R fr[6] = {f[5], f[4], f[3], f[2], f[1], f[0]};
-        if (interp == 0) { UL[n] = weno5_fwd(f); UR[n] = weno5_fwd(fr); }
-        else {
-            R a = R(0), b = R(0);
-#pragma unroll
-            for (int m = 0; m < 6; ++m) { a += lin[m] * f[m]; b += lin[m] * fr[m]; }
-            UL[n] = a; UR[n] = b;
-        }
-    }
+    for (int n = 0; n < 5; ++n) interp_pair_fwd<R, INTERP>(U[n], lin, hd, UL[n], UR[n]);
     R ULb[5] = {0, 0, 0, 0, 0}, URb[5] = {0, 0, 0, 0, 0};
-    if (riemann == 0) roe_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
-    else if (riemann == 1) rusanov_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
-    else hll_vjp<DIR, R>(UL, UR, g, Fb, ULb, URb);
+    riemann_vjp<DIR, R, RS>(UL, UR, g, Fb, ULb, URb);
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
-        const R *f = U[n];
-        if (interp == 0) {
-            R fbl[5] = {0, 0, 0, 0, 0};
-            weno5_vjp(f, ULb[n], fbl);
+        R gb[6];
+        interp_pair_vjp<R, INTERP>(U[n], lin, hd, ULb[n], URb[n], gb);
 #pragma unroll
-            for (int m = 0; m < 5; ++m) Ub[n][m] += fbl[m];
-            R fr[5] = {f[5], f[4], f[3], f[2], f[1]};
-            R fbr[5] = {0, 0, 0, 0, 0};
-            weno5_vjp(fr, URb[n], fbr);
-#pragma unroll
-            for (int m = 0; m < 5; ++m) Ub[n][5 - m] += fbr[m];
-        } else {
-#pragma unroll
-            for (int m = 0; m < 6; ++m) Ub[n][m] += lin[m] * ULb[n] + lin[5 - m] * URb[n];
-        }
+        for (int m = 0; m < 6; ++m) Ub[n][m] += gb[m];
     }
 }
 
-// run-time selection (interp 0 WENO5 / 2 MDCD_LINEAR; riemann 0 Roe, 1 Rusanov, 2 HLL)
+// run-time selection (interp 0 WENO5 / 2 MDCD_LINEAR / 3 MDCD_HYBRID; rcode a
+// riemann_vjp code)
+template <int DIR, typename R, int INTERP>
+NS3D_HD void face_vjp_i(int rcode, const R *lin, const R *hd, R g, const R U[5][6], const R *Fb, R Ub[5][6]) {
+    if (rcode == 0) face_vjp_t<DIR, R, INTERP, 0>(lin, hd, g, U, Fb, Ub);
+    else if (rcode == 1) face_vjp_t<DIR, R, INTERP, 1>(lin, hd, g, U, Fb, Ub);
+    else if (rcode == 2) face_vjp_t<DIR, R, INTERP, 2>(lin, hd, g, U, Fb, Ub);
+    else face_vjp_t<DIR, R, INTERP, 3>(lin, hd, g, U, Fb, Ub);
+}
+
 template <int DIR, typename R>
-NS3D_HD void face_vjp(int interp, int riemann, const R *lin, R g, const R U[5][6], const R *Fb, R Ub[5][6]) {
-    if (interp == 0) {
-        if (riemann == 0) face_vjp_t<DIR, R, 0, 0>(lin, g, U, Fb, Ub);
-        else if (riemann == 1) face_vjp_t<DIR, R, 0, 1>(lin, g, U, Fb, Ub);
-        else face_vjp_t<DIR, R, 0, 2>(lin, g, U, Fb, Ub);
-    } else {
-        if (riemann == 0) face_vjp_t<DIR, R, 2, 0>(lin, g, U, Fb, Ub);
-        else if (riemann == 1) face_vjp_t<DIR, R, 2, 1>(lin, g, U, Fb, Ub);
-        else face_vjp_t<DIR, R, 2, 2>(lin, g, U, Fb, Ub);
-    }
+NS3D_HD void face_vjp(int interp, int rcode, const R *lin, const R *hd, R g, const R U[5][6], const R *Fb,
+                      R Ub[5][6]) {
+    if (interp == 0) face_vjp_i<DIR, R, 0>(rcode, lin, hd, g, U, Fb, Ub);
+    else if (interp == 2) face_vjp_i<DIR, R, 2>(rcode, lin, hd, g, U, Fb, Ub);
+    else face_vjp_i<DIR, R, 3>(rcode, lin, hd, g, U, Fb, Ub);
 }
 
 // ------------------------------------------------------------ viscous VJP

@@ -17,8 +17,9 @@ struct AdjArgs {
     Layout L;
     double inv_h[3];
     double gamma, Rgas, mu0, S, cpr;
-    int interp, riemann;
-    double lin[6];
+    int interp, riemann;  // public values (NS3D_WENO5 ... ; NS3D_ROE ...)
+    double lin[6];        // MDCD linear coefficients
+    double hd[4];         // MDCD_HYBRID WENO weights d0..d3
     int first;            // 1: the x-direction gather overwrites Ub
 };
 

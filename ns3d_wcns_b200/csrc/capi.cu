@@ -755,12 +755,13 @@ bool adjoint_supported(const ns3d_handle *h, std::string &why) {
         why = "adjoint: periodic boundaries in all directions only"; return false;
     }
     if (h->P.char_recon) { why = "adjoint: component-wise interpolation only"; return false; }
-    if (h->P.interpolation != NS3D_WENO5 && h->P.interpolation != NS3D_MDCD_LINEAR) {
-        why = "adjoint: WENO5 or MDCD_LINEAR interpolation only"; return false;
+    if (h->P.interpolation != NS3D_WENO5 && h->P.interpolation != NS3D_MDCD_LINEAR &&
+        h->P.interpolation != NS3D_MDCD_HYBRID) {
+        why = "adjoint: WENO5, MDCD_LINEAR or MDCD_HYBRID interpolation only"; return false;
     }
     const int rs = h->P.riemann_solver;
-    if (rs != NS3D_ROE && rs != NS3D_RUSANOV && rs != NS3D_HLL) {
-        why = "adjoint: Roe, Rusanov or HLL flux only"; return false;
+    if (rs != NS3D_ROE && rs != NS3D_RUSANOV && rs != NS3D_HLL && rs != NS3D_HLLC) {
+        why = "adjoint: Roe, Rusanov, HLL or HLLC flux only"; return false;
     }
     return true;
 }
@@ -799,6 +800,7 @@ AdjArgs adj_args(ns3d_handle *h, double *const W[5], const double *const Rb[5], 
     a.gamma = h->ph.gamma; a.Rgas = h->ph.Rgas; a.mu0 = h->ph.mu; a.S = h->ph.S; a.cpr = h->ph.Cp / h->ph.Pr;
     a.interp = h->P.interpolation; a.riemann = h->P.riemann_solver == NS3D_HLL ? 3 : h->P.riemann_solver;
     for (int m = 0; m < 6; ++m) a.lin[m] = h->sp64.lin[m];
+    for (int m = 0; m < 4; ++m) a.hd[m] = h->sp64.hd[m];
     a.first = 0;
     a.rbs = 1.0;
     return a;

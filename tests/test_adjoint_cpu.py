@@ -37,14 +37,21 @@ def random_stencil(rng, jump=False):
 
 
 LIN = np.array([0.0248, -0.2015, 0.6952, 0.5734, -0.0848, -0.0071])
+# MDCD_HYBRID's WENO weights d0..d3 for mdcd_disp 0.0463783, mdcd_diss 0.01
+# (interpolation.cpp:179-182), appended to the linear coefficients
+HD = np.array([1.5 * (0.0463783 + 0.01), 0.5 - 1.5 * (0.0463783 - 0.03), 0.5 - 1.5 * (0.0463783 + 0.03),
+               1.5 * (0.0463783 - 0.01)])
 
 
 @pytest.mark.parametrize("direction", [0, 1, 2])
-@pytest.mark.parametrize("interp", [0, 2])
-@pytest.mark.parametrize("riemann", [0, 1, 3])
+@pytest.mark.parametrize("interp", [0, 2, 3])
+@pytest.mark.parametrize("riemann", [0, 1, 2, 3])
 def test_face_vjp_matches_finite_differences(lib, direction, interp, riemann):
+    """Roe, Rusanov, HLLC (public value 2) and HLL (3) with WENO5,
+    MDCD_LINEAR and MDCD_HYBRID (detector switch: zero derivative, active
+    branch differentiated)."""
     rng = np.random.default_rng(100 * direction + 10 * interp + riemann)
-    lin = np.ascontiguousarray(LIN)
+    lin = np.ascontiguousarray(np.concatenate([LIN, HD]))
     worst, kinks = 0.0, 0
 
     def fd(U, dU, Fb, h):

@@ -38,7 +38,9 @@ def embed(x_int, shape):
     return out
 
 
-SCHEMES = [(0, 0), (2, 1), (0, 3)]  # (interpolation, riemann): WENO5+Roe, MDCD_LINEAR+Rusanov, WENO5+HLL
+# (interpolation, riemann): WENO5+Roe, MDCD_LINEAR+Rusanov, WENO5+HLL, and the benchmark
+# scheme MDCD_HYBRID+HLLC (the detector a switch: zero derivative, active branch differentiated)
+SCHEMES = [(0, 0), (2, 1), (0, 3), (3, 2), (2, 2)]
 
 
 def setup(n, interp, rs, Re=200.0):
@@ -71,7 +73,7 @@ def test_vjp_rhs_dot_product(gpu_lib, scheme, n):
         assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
 
 
-@pytest.mark.parametrize("scheme", SCHEMES[:2])
+@pytest.mark.parametrize("scheme", SCHEMES[:2] + SCHEMES[3:])
 def test_vjp_rk3_step_dot_product(gpu_lib, scheme):
     n = (12, 12, 12)
     s, P, G, st = setup(n, *scheme)
@@ -96,11 +98,12 @@ def test_vjp_rk3_step_dot_product(gpu_lib, scheme):
         assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
 
 
-def test_kinetic_energy_gradient_against_fd(gpu_lib):
+@pytest.mark.parametrize("scheme", [(0, 0), (2, 2)], ids=["weno5_roe", "mdcd_linear_hllc"])
+def test_kinetic_energy_gradient_against_fd(gpu_lib, scheme):
     """Config-4 shape at reduced size: Re 200, dt 2e-3, checkpoints + recompute."""
     n = (16, 16, 16)
     nsteps, ce = 30, 7
-    s, P, G, st = setup(n, 0, 0)
+    s, P, G, st = setup(n, *scheme)
     rng = np.random.default_rng(9)
     with s:
         s.set_interior_primitives(*st)
