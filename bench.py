@@ -349,7 +349,7 @@ def batched_report(device: int, n: int = 512, check=((200, 8, "reference"), (400
                          f"(the GPU run's step counts) on {cores} cores"}
     return {"config": f"{n} shock tubes Nx x 4 x 4, Nx in {{200,400,800,1600}}, WENO5+Roe, CFL 0.5, t_end 0.14-0.2",
             "problems_per_s": n / wall, "wall_s": wall, "cell_updates_per_s": cell_updates / wall,
-            "autotuned": {"cluster": cfg[0], "threads": cfg[1]}, "steps_max": max(steps),
+            "autotuned": {"cluster": cfg[0], "threads": cfg[1], "ctas_per_sm": cfg[2]}, "steps_max": max(steps),
             "l1_vs_cpu": per_nx, "cpu_baseline": cpu}
 
 

@@ -244,7 +244,9 @@ int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int check
  * Plain FP64, inviscid (Re = inf), y and z periodic, any x boundary types,
  * component-wise interpolation.  Thread-block clusters take problems from an
  * atomic work queue, largest first; ns3d_batch_autotune times the cluster
- * size (1,2,4,8) x CTA width (128,256) choices and keeps the fastest. */
+ * size (1,2,4,8) x CTA width (128,256) x resident CTAs per SM (1,2,3: the
+ * register budget of the kernel instantiation) choices and keeps the
+ * fastest; config_out = {cluster, width, CTAs per SM}. */
 typedef struct ns3d_batch ns3d_batch;
 int ns3d_batch_create(const ns3d_params *params, int n_problems, const ns3d_grid *grids, const double *t_end,
                       ns3d_batch **out);
@@ -254,8 +256,8 @@ const char *ns3d_batch_last_error(const ns3d_batch *b);
 int ns3d_batch_set_interior_primitives(ns3d_batch *b, int problem, const double *const fields[5]);
 /* one persistent launch (captured in a CUDA graph) to every problem's t_end */
 int ns3d_batch_run(ns3d_batch *b, int max_steps);
-int ns3d_batch_autotune(ns3d_batch *b, int trial_steps, int config_out[2]);
-int ns3d_batch_set_config(ns3d_batch *b, int cluster, int threads);
+int ns3d_batch_autotune(ns3d_batch *b, int trial_steps, int config_out[3]);
+int ns3d_batch_set_config(ns3d_batch *b, int cluster, int threads, int ctas_per_sm);
 /* final time, steps taken, status (0 reached t_end, 1 dt <= 1e-12, 2 max_steps) */
 int ns3d_batch_query(ns3d_batch *b, int problem, double *time, int *steps, int *status);
 /* primitive Field3D arrays (rho,u,v,w,p; sx*sy*sz each) of problem i */

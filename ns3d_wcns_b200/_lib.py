@@ -107,7 +107,7 @@ def load() -> C.CDLL:
     lib.ns3d_batch_set_interior_primitives.argtypes = [h, C.c_int, C.POINTER(dp)]
     lib.ns3d_batch_run.argtypes = [h, C.c_int]
     lib.ns3d_batch_autotune.argtypes = [h, C.c_int, C.POINTER(C.c_int)]
-    lib.ns3d_batch_set_config.argtypes = [h, C.c_int, C.c_int]
+    lib.ns3d_batch_set_config.argtypes = [h, C.c_int, C.c_int, C.c_int]
     lib.ns3d_batch_query.argtypes = [h, C.c_int, dp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.ns3d_batch_download.argtypes = [h, C.c_int, C.POINTER(dp)]
     lib.ns3d_debug_face_vjp.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, dp, dp, dp, dp, dp]

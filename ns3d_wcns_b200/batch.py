@@ -64,12 +64,13 @@ class Batch:
         self._check(self.lib.ns3d_batch_run(self.h, int(max_steps)))
 
     def autotune(self, trial_steps: int = 20):
-        out = (C.c_int * 2)()
+        """(cluster size, CTA width, resident CTAs per SM) of the fastest trial."""
+        out = (C.c_int * 3)()
         self._check(self.lib.ns3d_batch_autotune(self.h, int(trial_steps), out))
-        return out[0], out[1]
+        return out[0], out[1], out[2]
 
-    def set_config(self, cluster: int, threads: int) -> None:
-        self._check(self.lib.ns3d_batch_set_config(self.h, int(cluster), int(threads)))
+    def set_config(self, cluster: int, threads: int, ctas_per_sm: int = 1) -> None:
+        self._check(self.lib.ns3d_batch_set_config(self.h, int(cluster), int(threads), int(ctas_per_sm)))
 
     def query(self, i: int):
         t, s, st = C.c_double(), C.c_int(), C.c_int()

@@ -46,8 +46,12 @@ struct Inst {
 };
 
 // per-problem array offsets relative to Inst::base (units of L.plane):
-// W buffers 0..14 (3 x 5), face fluxes X 15..19, Y 20..24, Z 25..29
-constexpr int NARR = 30;
+// W buffers 0..14 (3 x 5), face fluxes X 15..19, Y 20..24, Z 25..29, and the
+// conserved state U = p2c(W) of each W buffer 30..44 (every cell, ghosts
+// included), kept beside W so that each cell is converted once per stage
+// instead of once per stencil that reads it
+constexpr int NARR = 45;
+constexpr int UOFF = 30;
 
 struct BatchArgs {
     const Inst *inst;
@@ -69,9 +73,10 @@ __device__ __forceinline__ double *arr(const BatchArgs &a, const Inst &I, int q)
 }
 
 // Face flux of x-face g (between interior cells g-1 and g; g in [0, nx]) /
-// y-face, z-face g (between interior g and g+1, periodic wrap) of line (j,k)
-template <int DIR>
-__device__ __forceinline__ void face_flux(const BatchArgs &a, const Inst &I, const double *const *W, int g, int t1,
+// y-face, z-face g (between interior g and g+1, periodic wrap) of line (j,k),
+// from the stored conserved state U
+template <int DIR, int INTERP, int RS>
+__device__ __forceinline__ void face_flux(const BatchArgs &a, const Inst &I, const double *Uc, int g, int t1,
                                           int t2, double F[5]) {
     const Layout &L = I.L;
     const int n = DIR == 0 ? L.nx : (DIR == 1 ? L.ny : L.nz);
@@ -86,15 +91,16 @@ __device__ __forceinline__ void face_flux(const BatchArgs &a, const Inst &I, con
             if (c < NG) c += n; else if (c >= n + NG) c -= n;
         }
         long id = DIR == 0 ? L.at(c, t1, t2) : (DIR == 1 ? L.at(t1, c, t2) : L.at(t1, t2, c));
-        double U[5];
-        p2c_exact(W[0][id], W[1][id], W[2][id], W[3][id], W[4][id], a.gamma, U);
-        for (int q = 0; q < 5; ++q) st[q][m] = U[q];
+        for (int q = 0; q < 5; ++q) st[q][m] = Uc[(long)q * L.plane + id];
     }
     double wi[5] = {0, 0, 0, 0, 0};
-    wcns_face<DIR, double, RUNTIME, RUNTIME, 0>(a.sp, st, wi, wi, F);
+    wcns_face<DIR, double, INTERP, RS, 0>(a.sp, st, wi, wi, F);
 }
 
-__global__ void __launch_bounds__(256) batch_kernel(BatchArgs a) {
+// INTERP / RS: compile-time scheme (RUNTIME: from a.sp); MINB: resident CTAs
+// per SM the register allocation is sized for (one of the autotuned knobs)
+template <int INTERP, int RS, int MINB>
+__global__ void __launch_bounds__(256, MINB) batch_kernel(BatchArgs a) {
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank();
     const int csize = (int)cluster.num_blocks();
@@ -124,12 +130,29 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs a) {
         const Layout &L = I.L;
         // this CTA's share of the interior x range
         const int x0 = (int)((long)L.nx * crank / csize), x1 = (int)((long)L.nx * (crank + 1) / csize);
-        double *W[3][5];
-        for (int b = 0; b < 3; ++b)
-            for (int q = 0; q < 5; ++q) W[b][q] = arr(a, I, 5 * b + q);
-        double *FX[5], *FY[5], *FZ[5];
-        for (int q = 0; q < 5; ++q) { FX[q] = arr(a, I, 15 + q); FY[q] = arr(a, I, 20 + q); FZ[q] = arr(a, I, 25 + q); }
+        // the problem's arrays, addressed from one base (no pointer tables in
+        // registers): array q of the list in NARR's comment at base + q * plane
+        double *const P0 = a.pool + I.base;
+        const long pl = L.plane;
+        auto W = [&](int b, int q) { return P0 + (long)(5 * b + q) * pl; };
+        auto U = [&](int b, int q) { return P0 + (long)(UOFF + 5 * b + q) * pl; };
+        auto FX = [&](int q) { return P0 + (long)(15 + q) * pl; };
+        auto FY = [&](int q) { return P0 + (long)(20 + q) * pl; };
+        auto FZ = [&](int q) { return P0 + (long)(25 + q) * pl; };
         const int cells_yz = L.ny * L.nz;
+        // this CTA's share of the ghost-inclusive x range (the end CTAs take the x ghost slabs)
+        const int gx0 = crank == 0 ? 0 : x0 + NG, gx1 = crank == csize - 1 ? L.sx : x1 + NG;
+        const long gcells = (long)(gx1 - gx0) * L.sy * L.sz;
+        // conserved state of the initial buffer, every cell
+        for (long e = tid; e < gcells; e += nth) {
+            const int ci = gx0 + (int)(e % (gx1 - gx0));
+            const long r2 = e / (gx1 - gx0);
+            const long o = L.at(ci, (int)(r2 % L.sy), (int)(r2 / L.sy));
+            double Uo[5];
+            p2c_exact(W(0, 0)[o], W(0, 1)[o], W(0, 2)[o], W(0, 3)[o], W(0, 4)[o], a.gamma, Uo);
+            for (int q = 0; q < 5; ++q) U(0, q)[o] = Uo[q];
+        }
+        cluster.sync();
         int s0 = 0;
         double t = 0.0;
         int steps = 0, status = 2;
@@ -140,9 +163,8 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs a) {
             for (long e = tid; e < (long)(x1 - x0) * cells_yz; e += nth) {
                 const int i = x0 + (int)(e % (x1 - x0)), jk = (int)(e / (x1 - x0));
                 const long c = L.at(i + NG, jk % L.ny + NG, jk / L.ny + NG);
-                double U[5];
-                p2c_exact(W[s0][0][c], W[s0][1][c], W[s0][2][c], W[s0][3][c], W[s0][4][c], a.gamma, U);
-                m = fmin(m, cfl_bound(U, a.gamma, I.dx));
+                const double Us[5] = {U(s0, 0)[c], U(s0, 1)[c], U(s0, 2)[c], U(s0, 3)[c], U(s0, 4)[c]};
+                m = fmin(m, cfl_bound(Us, a.gamma, I.dx));
             }
             block_min_any(m, &a.partials[(long)pi * 16 + crank]);
             cluster.sync();
@@ -157,26 +179,26 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs a) {
             for (int stage = 1; stage <= 3; ++stage) {
                 const int src = stage == 1 ? s0 : (stage == 2 ? b1 : b2);
                 const int dst = stage == 2 ? b2 : b1;
-                const double *const *Wc = W[src];
+                const double *const Uc = U(src, 0);
                 // faces: x-faces g in [x0, x1) (+ g = nx for the last CTA), y/z faces per column
                 const int gx_hi = (crank == csize - 1) ? x1 + 1 : x1;
                 for (long e = tid; e < (long)(gx_hi - x0) * cells_yz; e += nth) {
                     const int g = x0 + (int)(e % (gx_hi - x0)), jk = (int)(e / (gx_hi - x0));
                     const int j = jk % L.ny, k = jk / L.ny;
                     double F[5];
-                    face_flux<0>(a, I, Wc, g, j + NG, k + NG, F);
+                    face_flux<0, INTERP, RS>(a, I, Uc, g, j + NG, k + NG, F);
                     const long o = ((long)k * L.ny + j) * (L.nx + 1) + g;
-                    for (int q = 0; q < 5; ++q) FX[q][o] = F[q];
+                    for (int q = 0; q < 5; ++q) FX(q)[o] = F[q];
                 }
                 for (long e = tid; e < (long)(x1 - x0) * cells_yz; e += nth) {
                     const int i = x0 + (int)(e % (x1 - x0)), jk = (int)(e / (x1 - x0));
                     const int j = jk % L.ny, k = jk / L.ny;
                     double F[5];
                     const long o = ((long)k * L.ny + j) * L.nx + i;
-                    face_flux<1>(a, I, Wc, j, i + NG, k + NG, F);
-                    for (int q = 0; q < 5; ++q) FY[q][o] = F[q];
-                    face_flux<2>(a, I, Wc, k, i + NG, j + NG, F);
-                    for (int q = 0; q < 5; ++q) FZ[q][o] = F[q];
+                    face_flux<1, INTERP, RS>(a, I, Uc, j, i + NG, k + NG, F);
+                    for (int q = 0; q < 5; ++q) FY(q)[o] = F[q];
+                    face_flux<2, INTERP, RS>(a, I, Uc, k, i + NG, j + NG, F);
+                    for (int q = 0; q < 5; ++q) FZ(q)[o] = F[q];
                 }
                 cluster.sync();
                 // RHS + stage update of this CTA's interior cells
@@ -188,7 +210,7 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs a) {
                         auto fx = [&](int g) -> double {
                             if (g < 0) { if (I.bc[0] == BC_OUTFLOW) g = 0; else return 0.0; }
                             if (g > L.nx) { if (I.bc[1] == BC_OUTFLOW) g = L.nx; else return 0.0; }
-                            return FX[q][((long)k * L.ny + j) * (L.nx + 1) + g];
+                            return FX(q)[((long)k * L.ny + j) * (L.nx + 1) + g];
                         };
                         // cell i uses faces i-3 .. i+2 (ghost-inclusive), x-face g = f - (NG - 1)
                         auto dh = [](double f0, double f1, double f2, double f3, double f4, double f5, double ih) {
@@ -197,11 +219,11 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs a) {
                         double r = 0.0 - dh(fx(i - 2), fx(i - 1), fx(i), fx(i + 1), fx(i + 2), fx(i + 3), I.inv_dx);
                         auto fy = [&](int jj) {
                             jj = jj < 0 ? jj + L.ny : (jj >= L.ny ? jj - L.ny : jj);
-                            return FY[q][((long)k * L.ny + jj) * L.nx + i];
+                            return FY(q)[((long)k * L.ny + jj) * L.nx + i];
                         };
                         auto fz = [&](int kk) {
                             kk = kk < 0 ? kk + L.nz : (kk >= L.nz ? kk - L.nz : kk);
-                            return FZ[q][((long)kk * L.ny + j) * L.nx + i];
+                            return FZ(q)[((long)kk * L.ny + j) * L.nx + i];
                         };
                         // periodic y/z: face jj + 1/2 between interior jj and jj+1; cell j uses jj = j-3 .. j+2
                         r = r - dh(fy(j - 3), fy(j - 2), fy(j - 1), fy(j), fy(j + 1), fy(j + 2), I.inv_dy);
@@ -209,19 +231,16 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs a) {
                         R[q] = r;
                     }
                     const long c = L.at(i + NG, j + NG, k + NG);
-                    double U0[5], U[5], Un[5], Wn[5];
-                    p2c_exact(W[s0][0][c], W[s0][1][c], W[s0][2][c], W[s0][3][c], W[s0][4][c], a.gamma, U0);
-                    if (stage == 1) for (int q = 0; q < 5; ++q) U[q] = U0[q];
-                    else p2c_exact(Wc[0][c], Wc[1][c], Wc[2][c], Wc[3][c], Wc[4][c], a.gamma, U);
-                    for (int q = 0; q < 5; ++q) Un[q] = rk_combine(stage, U0[q], U[q], R[q], dt);
+                    double Un[5], Wn[5], Ud[5];
+                    for (int q = 0; q < 5; ++q) Un[q] = rk_combine(stage, U(s0, q)[c], Uc[q * pl + c], R[q], dt);
                     c2p_exact(Un, a.gamma, Wn);
-                    for (int q = 0; q < 5; ++q) W[dst][q][c] = Wn[q];
+                    // runge_kutta_3's c2p -> p2c round trip: the stored conserved state is p2c(W)
+                    p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
+                    for (int q = 0; q < 5; ++q) { W(dst, q)[c] = Wn[q]; U(dst, q)[c] = Ud[q]; }
                 }
                 cluster.sync();
                 // ghost fill of the new state: cells in this CTA's x range (and the x ghost
                 // slabs for the end CTAs) that are not interior
-                const int gx0 = crank == 0 ? 0 : x0 + NG, gx1 = crank == csize - 1 ? L.sx : x1 + NG;
-                const long gcells = (long)(gx1 - gx0) * L.sy * L.sz;
                 BcInfo b;
                 for (int d = 0; d < 3; ++d) b.periodic[d] = I.periodic[d];
                 for (int f = 0; f < 6; ++f) b.bc[f] = I.bc[f];
@@ -238,20 +257,19 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchArgs a) {
                         special_state(kind, Wn);
                     } else if (is_interior(L, cc)) {
                         const long s = L.at(cc[0], cc[1], cc[2]);
-                        for (int q = 0; q < 5; ++q) Wn[q] = W[dst][q][s];
+                        for (int q = 0; q < 5; ++q) Wn[q] = W(dst, q)[s];
                     } else {
                         // a ghost cell no fill reaches keeps its own stage update with rhs = 0
                         const long s = L.at(cc[0], cc[1], cc[2]);
-                        double U0[5], U[5], Un[5];
-                        p2c_exact(W[s0][0][s], W[s0][1][s], W[s0][2][s], W[s0][3][s], W[s0][4][s], a.gamma, U0);
-                        if (stage == 1) for (int q = 0; q < 5; ++q) U[q] = U0[q];
-                        else p2c_exact(Wc[0][s], Wc[1][s], Wc[2][s], Wc[3][s], Wc[4][s], a.gamma, U);
-                        for (int q = 0; q < 5; ++q) Un[q] = rk_combine(stage, U0[q], U[q], 0.0, dt);
+                        double Un[5];
+                        for (int q = 0; q < 5; ++q) Un[q] = rk_combine(stage, U(s0, q)[s], Uc[q * pl + s], 0.0, dt);
                         c2p_exact(Un, a.gamma, Wn);
                     }
                     apply_flips(flip, Wn);
                     const long o = L.at(ci, cj, ck);
-                    for (int q = 0; q < 5; ++q) W[dst][q][o] = Wn[q];
+                    double Ud[5];
+                    p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
+                    for (int q = 0; q < 5; ++q) { W(dst, q)[o] = Wn[q]; U(dst, q)[o] = Ud[q]; }
                 }
                 cluster.sync();
             }
@@ -308,7 +326,7 @@ struct ns3d_batch {
     double **d_tab = nullptr;    // scratch pointer table (10 pointers)
     cudaStream_t stream = nullptr;
     int device = 0;
-    int cluster = 4, threads = 256;
+    int cluster = 4, threads = 256, minb = 1;
     cudaGraphExec_t graph = nullptr;
     int graph_max_steps = -1;
     SchemeParams<double> sp;
@@ -338,10 +356,25 @@ BatchArgs batch_args(ns3d_batch *b, int max_steps) {
     return a;
 }
 
-int launch_batch(ns3d_batch *b, int max_steps, int cluster, int threads) {
+typedef void (*BatchKernel)(BatchArgs);
+
+// the instantiation for the scheme and the resident-CTA target: WENO5 + Roe
+// (the shock-tube benchmark) compiled in, any other pair selected at run time
+template <int MINB>
+BatchKernel batch_kernel_for(const SchemeParams<double> &sp) {
+    if (sp.interp == I_WENO5 && sp.riemann == R_ROE) return batch_kernel<I_WENO5, R_ROE, MINB>;
+    return batch_kernel<RUNTIME, RUNTIME, MINB>;
+}
+
+BatchKernel select_kernel(const SchemeParams<double> &sp, int minb) {
+    return minb >= 3 ? batch_kernel_for<3>(sp) : (minb == 2 ? batch_kernel_for<2>(sp) : batch_kernel_for<1>(sp));
+}
+
+int launch_batch(ns3d_batch *b, int max_steps, int cluster, int threads, int minb) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     BatchArgs a = batch_args(b, max_steps);
+    const BatchKernel kern = select_kernel(b->sp, minb);
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -353,14 +386,14 @@ int launch_batch(ns3d_batch *b, int max_steps, int cluster, int threads) {
     // persistent grid: as many clusters as fit at once (clusters pull work)
     int max_clusters = 0;
     cfg.gridDim = dim3(cluster * sms);
-    if (cudaOccupancyMaxActiveClusters(&max_clusters, batch_kernel, &cfg) != cudaSuccess || max_clusters < 1) {
+    if (cudaOccupancyMaxActiveClusters(&max_clusters, (void *)kern, &cfg) != cudaSuccess || max_clusters < 1) {
         cudaGetLastError();
         max_clusters = std::max(1, sms / cluster);
     }
     const int nclusters = std::min(max_clusters, b->n);
     cfg.gridDim = dim3(cluster * std::max(1, nclusters));
     BCK(b, cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream), "counter reset");
-    BCK(b, cudaLaunchKernelEx(&cfg, batch_kernel, a), "batch launch");
+    BCK(b, cudaLaunchKernelEx(&cfg, kern, a), "batch launch");
     return NS3D_OK;
 }
 
@@ -505,7 +538,7 @@ int ns3d_batch_run(ns3d_batch *b, int max_steps) {
         if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
         cudaGraph_t g;
         BCK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "capture");
-        int r = launch_batch(b, max_steps, b->cluster, b->threads);
+        int r = launch_batch(b, max_steps, b->cluster, b->threads, b->minb);
         cudaError_t e = cudaStreamEndCapture(b->stream, &g);
         if (r) return r;
         if (e != cudaSuccess) return bfail(b, NS3D_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
@@ -522,37 +555,49 @@ int ns3d_batch_run(ns3d_batch *b, int max_steps) {
 int ns3d_batch_autotune(ns3d_batch *b, int trial_steps, int out[2]) {
     if (!b || trial_steps < 1) return NS3D_ERR_INVALID_ARG;
     cudaSetDevice(b->device);
-    // save the state, try each configuration for trial_steps steps, restore
-    std::vector<char> save(b->pool_bytes);
-    BCK(b, cudaMemcpy(save.data(), b->pool, b->pool_bytes, cudaMemcpyDeviceToHost), "save");
-    const int clusters[4] = {1, 2, 4, 8}, widths[2] = {128, 256};
+    // save the state (a device copy), try each configuration for trial_steps
+    // steps -- cluster size, CTA width and resident CTAs per SM (the register
+    // budget of the instantiation) -- and restore
+    double *save = nullptr;
+    BCK(b, cudaMalloc(&save, b->pool_bytes), "autotune save buffer");
+    cudaError_t se = cudaMemcpyAsync(save, b->pool, b->pool_bytes, cudaMemcpyDeviceToDevice, b->stream);
+    if (se != cudaSuccess) { cudaFree(save); return bfail(b, NS3D_ERR_CUDA, "autotune save"); }
+    const int clusters[4] = {1, 2, 4, 8}, widths[2] = {128, 256}, minbs[3] = {1, 2, 3};
     float best = 1e30f;
-    int bc = b->cluster, bw = b->threads;
+    int bc = b->cluster, bw = b->threads, bm = b->minb;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0); cudaEventCreate(&e1);
     for (int ci = 0; ci < 4; ++ci)
-        for (int wi = 0; wi < 2; ++wi) {
-            BCK(b, cudaMemcpy(b->pool, save.data(), b->pool_bytes, cudaMemcpyHostToDevice), "restore");
-            cudaEventRecord(e0, b->stream);
-            int r = launch_batch(b, trial_steps, clusters[ci], widths[wi]);
-            cudaEventRecord(e1, b->stream);
-            if (r || cudaStreamSynchronize(b->stream) != cudaSuccess) { cudaGetLastError(); continue; }
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best) { best = ms; bc = clusters[ci]; bw = widths[wi]; }
-        }
+        for (int wi = 0; wi < 2; ++wi)
+            for (int mi = 0; mi < 3; ++mi) {
+                if (cudaMemcpyAsync(b->pool, save, b->pool_bytes, cudaMemcpyDeviceToDevice, b->stream) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                cudaEventRecord(e0, b->stream);
+                int r = launch_batch(b, trial_steps, clusters[ci], widths[wi], minbs[mi]);
+                cudaEventRecord(e1, b->stream);
+                if (r || cudaStreamSynchronize(b->stream) != cudaSuccess) { cudaGetLastError(); continue; }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) { best = ms; bc = clusters[ci]; bw = widths[wi]; bm = minbs[mi]; }
+            }
     cudaEventDestroy(e0); cudaEventDestroy(e1);
-    BCK(b, cudaMemcpy(b->pool, save.data(), b->pool_bytes, cudaMemcpyHostToDevice), "restore");
-    b->cluster = bc; b->threads = bw;
+    se = cudaMemcpyAsync(b->pool, save, b->pool_bytes, cudaMemcpyDeviceToDevice, b->stream);
+    if (se == cudaSuccess) se = cudaStreamSynchronize(b->stream);
+    cudaFree(save);
+    if (se != cudaSuccess) return bfail(b, NS3D_ERR_CUDA, "autotune restore");
+    b->cluster = bc; b->threads = bw; b->minb = bm;
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
-    if (out) { out[0] = bc; out[1] = bw; }
+    if (out) { out[0] = bc; out[1] = bw; out[2] = bm; }
     return NS3D_OK;
 }
 
-int ns3d_batch_set_config(ns3d_batch *b, int cluster, int threads) {
-    if (!b || (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8) || (threads != 128 && threads != 256))
+int ns3d_batch_set_config(ns3d_batch *b, int cluster, int threads, int ctas_per_sm) {
+    if (!b || (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8) || (threads != 128 && threads != 256) ||
+        ctas_per_sm < 1 || ctas_per_sm > 3)
         return NS3D_ERR_INVALID_ARG;
-    b->cluster = cluster; b->threads = threads;
+    b->cluster = cluster; b->threads = threads; b->minb = ctas_per_sm;
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
     return NS3D_OK;
 }

@@ -636,7 +636,7 @@ int rk_stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, doubl
         h->launches += 1;
         CK(h, cudaGetLastError(), "ghost kernel");
         if (stage == 3) {
-            const int gx = (h->L32.nx + SweepGeom<2>::NLINE - 1) / SweepGeom<2>::NLINE;
+            const int gx = (h->L32.nx + SweepGeom<2, float>::NLINE - 1) / SweepGeom<2, float>::NLINE;
             h->cfl_count = (long)gx * h->L32.ny;  // z-sweep blocks
             h->cfl_valid = true;
         }
@@ -675,7 +675,7 @@ int rk_stage_async(ns3d_handle *h, int stage, int src0, int srcc, int dst, doubl
     h->launches += 1;
     CK(h, cudaGetLastError(), "ghost kernel");
     if (stage == 3) {
-        const int gx = (h->L64.nx + SweepGeom<2>::NLINE - 1) / SweepGeom<2>::NLINE;
+        const int gx = (h->L64.nx + SweepGeom<2, double>::NLINE - 1) / SweepGeom<2, double>::NLINE;
         h->cfl_count = (long)gx * h->L64.ny;  // z-sweep blocks
         h->cfl_valid = true;
     }

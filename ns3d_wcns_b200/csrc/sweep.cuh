@@ -96,13 +96,21 @@ struct SweepArgs {
 // At the end of a chunk the tails are moved to the front and the staged next
 // cells appended, so every stencil read is a fixed offset from the thread's
 // own position.
-template <int DIR>
+// FP64 y/z chunk geometry (faces per chunk, lines per block; C * NLINE = 256)
+#ifndef NS3D_SWEEP64_YZ_C
+#define NS3D_SWEEP64_YZ_C 8
+#endif
+#ifndef NS3D_SWEEP64_YZ_NL
+#define NS3D_SWEEP64_YZ_NL 32
+#endif
+template <int DIR, typename R>
 struct SweepGeom {
-    static constexpr int C = DIR == 0 ? 32 : 8;        // faces per chunk
-    static constexpr int NLINE = DIR == 0 ? 8 : 32;    // lines per block
+    static constexpr bool F64 = sizeof(R) == 8;
+    static constexpr int C = DIR == 0 ? 32 : (F64 ? NS3D_SWEEP64_YZ_C : 8);        // faces per chunk
+    static constexpr int NLINE = DIR == 0 ? 8 : (F64 ? NS3D_SWEEP64_YZ_NL : 32);  // lines per block
     static constexpr int CH = C * NLINE;               // threads
     static constexpr int NU = C + 5, NF = C + 7, NV = C + 8;
-    // along x a warp owns one line ([line][pos]); along y/z the lanes span 32
+    // along x a warp owns one line ([line][pos]); along y/z the lanes span
     // neighbouring lines ([pos][line]); both are conflict-free
     template <int NP>
     __device__ __forceinline__ static int idx(int line, int pos) {
@@ -117,14 +125,17 @@ struct SweepGeom {
 // chunk's cells (true) or loaded into registers (false).
 constexpr bool kRoldSmem = true;
 // minimum resident blocks per SM requested from the register allocator
+#ifndef NS3D_SWEEP64_MINB
+#define NS3D_SWEEP64_MINB 2
+#endif
 template <int DIR, typename R>
-constexpr int sweep_min_blocks() { return 2; }
+constexpr int sweep_min_blocks() { return sizeof(R) == 8 ? NS3D_SWEEP64_MINB : 2; }
 
 // buffers U(5) F(5) V(4) [W(5) for characteristic bases], staging W(5)+V(4)
 // [+ old RHS(5)]
 template <int DIR, typename R, bool CHARW>
 constexpr size_t sweep_smem_bytes() {
-    using G = SweepGeom<DIR>;
+    using G = SweepGeom<DIR, R>;
     return sizeof(R) * ((size_t)G::NLINE * (5 * G::NU + 5 * G::NF + 4 * G::NV + (CHARW ? 5 * G::NU : 0)) +
                         (size_t)(kRoldSmem ? 14 : 9) * G::CH) +
            (DIR == 2 ? (size_t)5 * G::CH * (sizeof(double) + (sizeof(R) == 4 ? sizeof(float) : 0)) : 0);  // fused stage
@@ -189,7 +200,7 @@ __device__ __forceinline__ void fused_stage_cell(const FusedStage &f, double dt,
 template <int DIR, typename R, int INTERP, int RS, int CHAR>
 __global__ void __launch_bounds__(256, sweep_min_blocks<DIR, R>())
 sweep_kernel(SweepArgs<R> a) {
-    using G = SweepGeom<DIR>;
+    using G = SweepGeom<DIR, R>;
     constexpr int C = G::C, NL = G::NLINE, CH = G::CH, NU = G::NU, NF = G::NF, NV = G::NV;
     constexpr bool USE_W = (CHAR != 0);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -690,7 +701,7 @@ sweep_kernel(SweepArgs<R> a) {
 
 template <int DIR, typename R, int INTERP, int RS, int CHAR>
 inline cudaError_t launch_sweep(const SweepArgs<R> &a, cudaStream_t st) {
-    using G = SweepGeom<DIR>;
+    using G = SweepGeom<DIR, R>;
     dim3 block(DIR == 0 ? G::C : G::NLINE, DIR == 0 ? G::NLINE : G::C);
     dim3 grid;
     if (DIR == 0) grid = dim3((a.L.ny + G::NLINE - 1) / G::NLINE, a.zhi - a.zlo);

@@ -187,7 +187,7 @@ struct PairGeom {
         return DIR == 0 ? pair * C + slot : slot * NP + pair;
     }
 };
-static_assert(PairGeom<2>::NL == SweepGeom<2>::NLINE, "the fused stage's CFL partials assume one z-sweep grid");
+static_assert(PairGeom<2>::NL == SweepGeom<2, float>::NLINE, "the fused stage's CFL partials assume one z-sweep grid");
 
 // float2 units: U(5) F(5) V(4), staging W(5)+V(4), old RHS(5); z-sweep:
 // FP64 U0 (5 double2), the FP32 stage increments (5 float2) and the deferred

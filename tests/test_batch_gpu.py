@@ -73,7 +73,7 @@ def test_batch_matches_oracle_per_problem(gpu_lib, scheme):
 def test_batch_results_do_not_depend_on_launch_config(gpu_lib):
     P, grids, states, t_end = problems()
     outs = []
-    for cfg in [(1, 128), (4, 256), (8, 128)]:
+    for cfg in [(1, 128, 1), (4, 256, 2), (8, 128, 3), (2, 256, 3)]:
         with Batch(P, grids, t_end) as b:
             for i, st in enumerate(states):
                 b.set_interior_primitives(i, *st)
@@ -90,8 +90,8 @@ def test_autotune_picks_a_valid_config_and_keeps_the_state(gpu_lib):
     with Batch(P, grids, t_end) as b:
         for i, st in enumerate(states):
             b.set_interior_primitives(i, *st)
-        cl, th = b.autotune(trial_steps=5)
-        assert cl in (1, 2, 4, 8) and th in (128, 256)
+        cl, th, mb = b.autotune(trial_steps=5)
+        assert cl in (1, 2, 4, 8) and th in (128, 256) and mb in (1, 2, 3)
         b.run()
         W, t, steps = oracle_run(P, grids[0], states[0], t_end[0])
         assert max(rel_linf(a, r) for a, r in zip(b.primitives(0), W)) <= 1e-10
