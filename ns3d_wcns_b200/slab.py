@@ -185,6 +185,11 @@ class SlabSolver:
         Gl.dz = G.dz
         self.P, self.Gl = Pl, Gl
         self.s = Solver(Pl, Gl, device=device)
+        # the stages and the halo moves must be ordered: the handle runs on the
+        # caller's current stream, which torch's copies and NCCL operations
+        # also follow
+        import torch
+        self.s.set_stream(torch.cuda.current_stream(device).cuda_stream)
         if plan.world > 1:
             # the global spacing, bit for bit (Lz / nz of the local extent may round differently)
             self.s._check(self.s.lib.ns3d_set_slab(self.s.h, plan.zlo, plan.zhi, float(G.dz)))
