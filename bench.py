@@ -205,15 +205,18 @@ def adjoint_report(device: int, n: int = 64, nsteps: int = 200, dt: float = 2e-3
         s.set_interior_primitives(*st)
         J2, grad2, stats2 = s.adjoint_kinetic_energy(nsteps, dt, ce)  # warm timing
         # the plain forward pass of the same steps (no checkpoint copies), device-timed
+        # on the handle's stream
         import torch
+        stream = torch.cuda.Stream()
+        s.set_stream(stream.cuda_stream)
         s.set_interior_primitives(*st)
         s.rk3_steps(2, dt)
         s.set_interior_primitives(*st)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        e0.record(stream)
         s.rk3_steps(nsteps, dt)
-        e1.record()
+        e1.record(stream)
         torch.cuda.synchronize()
         plain_forward_ms = e0.elapsed_time(e1)
         errs, errs4, noise, errsn = [], [], [], []
@@ -509,9 +512,8 @@ def run_slabs(args, rank, world, local, dist):
     P, G = bench_params(n, 0)
     plan = slab_plan(n, world, rank, periodic=True)
     st = isotropic_state((n, n, n), 1.4, 0.3, seed=0)  # one global field, every rank takes its planes
-    stream = torch.cuda.current_stream()
     sv = SlabSolver(P, G, plan, device=local)
-    sv.s.set_stream(stream.cuda_stream)
+    stream = sv.stream  # the handle's kernels, the halo exchange and the events share it
     local_st = [np.ascontiguousarray(sv.local_block(f)) for f in st]
     del st
     sv.s.set_interior_primitives(*local_st)
@@ -653,7 +655,9 @@ def main():
         cpu = cpu_baseline()
 
     st = isotropic_state((n, n, n), 1.4, 0.3, seed=rank)
-    stream = torch.cuda.current_stream()
+    # an explicit stream: the handles launch on it and the events are recorded on it
+    # (ns3d_set_stream with the default stream's NULL would give a handle a private stream)
+    stream = torch.cuda.Stream()
 
     def barrier():
         if dist is not None:

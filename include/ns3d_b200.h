@@ -195,7 +195,11 @@ int ns3d_time_advance(ns3d_handle *h, double t_end, int max_steps, double *time,
  * Pointers stay valid until the next ns3d_rk3_step / ns3d_destroy. */
 int ns3d_device_fields(ns3d_handle *h, int what, void *ptrs[5], long layout[6]);
 
-/* Bind the handle to a caller stream (cudaStream_t as void*; NULL = own). */
+/* Bind the handle to a caller stream (cudaStream_t as void*).  NULL gives the
+ * handle a private non-blocking stream of its own, not the legacy default
+ * stream: a caller that orders its own work with the handle's (copies of
+ * device_fields, NCCL operations, events) passes an explicit stream, e.g.
+ * a torch.cuda.Stream(), never torch's default stream (whose handle is 0). */
 int ns3d_set_stream(ns3d_handle *h, void *stream);
 int ns3d_synchronize(ns3d_handle *h);
 

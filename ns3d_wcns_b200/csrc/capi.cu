@@ -498,10 +498,14 @@ int visc_launch(ns3d_handle *h, double *red, long *nblocks = nullptr) {
     for (int q = 0; q < 3; ++q) maps.m[q] = sizeof(R) == 8 ? h->tmW64[h->s0][q] : h->tmW32[q];
     maps.m[3] = sizeof(R) == 8 ? h->tmT64 : h->tmT32;
     prof_begin(h, "viscous_flux");
-    if (va.periodic[0] && va.periodic[1] && va.periodic[2])
-        viscous_flux_kernel<R, true><<<g, dim3(VTX, VTY), 0, h->stream>>>(va, maps);
-    else
-        viscous_flux_kernel<R, false><<<g, dim3(VTX, VTY), 0, h->stream>>>(va, maps);
+    const bool p6 = va.periodic[0] && va.periodic[1] && va.periodic[2];
+    if (red) {
+        if (p6) viscous_flux_kernel<R, true, true><<<g, dim3(VTX, VTY), 0, h->stream>>>(va, maps);
+        else viscous_flux_kernel<R, false, true><<<g, dim3(VTX, VTY), 0, h->stream>>>(va, maps);
+    } else {
+        if (p6) viscous_flux_kernel<R, true, false><<<g, dim3(VTX, VTY), 0, h->stream>>>(va, maps);
+        else viscous_flux_kernel<R, false, false><<<g, dim3(VTX, VTY), 0, h->stream>>>(va, maps);
+    }
     prof_end(h);
     h->launches += 1;
     CK(h, cudaGetLastError(), "viscous kernel");
@@ -1523,12 +1527,10 @@ int ns3d_diagnostics(ns3d_handle *h, double out[6]) {
     const double vol = h->ph.dx * h->ph.dy * h->ph.dz;
     double s[5];
     if (!h->mixed && h->ph.mu != 0.0 && !h->diag_separate) {
-        // fused: the viscous kernel of the current state -- the one the next
-        // RK stage (or compute_rhs) starts with, which then reuses its node
-        // fluxes -- adds up the sums as it forms the gradients
+        // the viscous kernel's gradient pass (TMA plane tiles, register
+        // windows) with the sums instead of the node fluxes
         long nb = 0;
         if ((r = visc_launch<double>(h, h->visc_red, &nb))) return r;
-        h->visc_valid = true;
         if ((r = reduce_combine(h, 5, 0, s, h->visc_red, nb))) return r;
         if ((r = check_device_error(h))) return r;
     } else if (!h->mixed) {

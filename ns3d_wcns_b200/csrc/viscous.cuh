@@ -126,7 +126,10 @@ constexpr int vtile_stride() {  // elements per tile, 128-byte aligned tiles
 // P6: every direction periodic, so every derivative is the 6th-order central
 // one (choose_scheme's order for periodic directions) and the order dispatch
 // compiles away.
-template <typename R, bool P6>
+// DIAG: the ns3d_diagnostics sums (a.red) from the same gradient tiles, and
+// no node fluxes; a separate instantiation, so the kernel of the RK stages
+// carries none of it.
+template <typename R, bool P6, bool DIAG>
 __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, const __grid_constant__ ViscMaps tm) {
     constexpr int TS = vtile_stride<R>();
     __shared__ __align__(128) R sm[2 * 4 * TS];  // two plane tiles of u, v, w, T
@@ -158,7 +161,7 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
     };
     unsigned phase = 0u;  // bit b: parity of buffer b's next completion
     if (tid == 0) issue(0, kb);
-    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ns3d_diagnostics sums (a.red)
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // ns3d_diagnostics sums (DIAG)
     // window: win[q][m] = value at interior plane k - 3 + m (ghost-inclusive k + m)
     R win[4][7], nxt[4];
 #pragma unroll
@@ -218,12 +221,14 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
             const R kq = mu * a.cp_over_pr;
             const R u = win[0][3], v = win[1][3], w = win[2][3];
             const long o = ((long)k * L.ny + j) * L.nx + i;
-            a.V[0][o] = txx; a.V[1][o] = tyy; a.V[2][o] = tzz;
-            a.V[3][o] = txy; a.V[4][o] = txz; a.V[5][o] = tyz;
-            a.V[6][o] = u * txx + v * txy + w * txz + kq * Tx;
-            a.V[7][o] = u * txy + v * tyy + w * tyz + kq * Ty;
-            a.V[8][o] = u * txz + v * tyz + w * tzz + kq * Tz;
-            if (a.red && k >= a.rlo && k < a.rhi) {
+            if (!DIAG) {
+                a.V[0][o] = txx; a.V[1][o] = tyy; a.V[2][o] = tzz;
+                a.V[3][o] = txy; a.V[4][o] = txz; a.V[5][o] = tyz;
+                a.V[6][o] = u * txx + v * txy + w * txz + kq * Tx;
+                a.V[7][o] = u * txy + v * tyy + w * tyz + kq * Ty;
+                a.V[8][o] = u * txz + v * tyz + w * tzz + kq * Tz;
+            }
+            if (DIAG && k >= a.rlo && k < a.rhi) {
                 const double rho = (double)a.W[0][col + (long)(k + NG) * zs];
                 const double du = u, dv = v, dw = w, uu = du * du + dv * dv + dw * dw;
                 acc[0] += 0.5 * rho * uu * a.vol;
@@ -244,7 +249,7 @@ __global__ void __launch_bounds__(VTX * VTY) viscous_flux_kernel(ViscArgs<R> a, 
             for (int q = 0; q < 4; ++q) win[q][m] = win[q][m + 1];
         __syncthreads();  // this tile's reads done before it is refilled
     }
-    if (a.red)  // uniform: every thread of the block arrives
+    if (DIAG)  // uniform: every thread of the block arrives
         block_sum_n<5, VTX * VTY>(acc, a.red + 5 * ((long)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x));
 }
 

@@ -167,7 +167,7 @@ class SlabSolver:
     copies between the handles)."""
 
     def __init__(self, P, G, plan: SlabPlan, device: int = 0, exchange_fn=None, allreduce_min=None,
-                 allreduce_sum=None):
+                 allreduce_sum=None, stream=None):
         from .config import BCType, GridDesc
         from .solver import Solver
         import copy
@@ -185,11 +185,13 @@ class SlabSolver:
         Gl.dz = G.dz
         self.P, self.Gl = Pl, Gl
         self.s = Solver(Pl, Gl, device=device)
-        # the stages and the halo moves must be ordered: the handle runs on the
-        # caller's current stream, which torch's copies and NCCL operations
-        # also follow
+        # the stages and the halo moves must be ordered: the handle and the
+        # torch copies / NCCL operations of the exchange run on one explicit
+        # (non-default) stream; ns3d_set_stream(NULL) would give the handle a
+        # private stream of its own
         import torch
-        self.s.set_stream(torch.cuda.current_stream(device).cuda_stream)
+        self.stream = stream if stream is not None else torch.cuda.Stream(device=device)
+        self.s.set_stream(self.stream.cuda_stream)
         if plan.world > 1:
             # the global spacing, bit for bit (Lz / nz of the local extent may round differently)
             self.s._check(self.s.lib.ns3d_set_slab(self.s.h, plan.zlo, plan.zhi, float(G.dz)))
@@ -216,18 +218,25 @@ class SlabSolver:
         return device_planes(self.s, k0, count)
 
     def exchange_halos(self) -> None:
-        self._exchange(self.plan, self.planes)
+        import torch
+        with torch.cuda.stream(self.stream):
+            self._exchange(self.plan, self.planes)
 
     # -- time advance
     launch_count = 0  # kernels this rank's handle launched (ns3d_last_launch_count summed)
 
     def compute_timestep(self) -> float:
+        import torch
         dt = self.s.compute_timestep()
         self.launch_count += self.s.launches()
-        return self._min(dt)
+        with torch.cuda.stream(self.stream):
+            return self._min(dt)
 
     def total_energy(self) -> float:
-        return self._sum(self.s.total_energy())
+        import torch
+        ke = self.s.total_energy()
+        with torch.cuda.stream(self.stream):
+            return self._sum(ke)
 
     def rk3_step(self, dt: float) -> None:
         for stage in (1, 2, 3):
@@ -257,11 +266,14 @@ class InProcessSlabs:
     against a single-domain run on one device."""
 
     def __init__(self, P, G, world: int, device: int = 0):
+        import torch
         periodic = P.bc_zmin == P.bc_zmax and int(P.bc_zmin) == 0
         self.plans = [slab_plan(G.global_nz, world, r, periodic) for r in range(world)]
         ident = lambda x: x
+        # one stream for every slab's kernels and for the copies between them
+        self.stream = torch.cuda.Stream(device=device)
         self.slabs = [SlabSolver(P, G, pl, device=device, exchange_fn=lambda *_: None, allreduce_min=ident,
-                                 allreduce_sum=ident) for pl in self.plans]
+                                 allreduce_sum=ident, stream=self.stream) for pl in self.plans]
 
     def close(self):
         for s in self.slabs:
@@ -278,6 +290,11 @@ class InProcessSlabs:
             s.set_interior_primitives(rho, u, v, w, p)
 
     def exchange_halos(self) -> None:
+        import torch
+        with torch.cuda.stream(self.stream):
+            self._copy_halos()
+
+    def _copy_halos(self) -> None:
         for s in self.slabs:
             pl = s.plan
             if pl.lower is not None:

@@ -38,11 +38,12 @@ def test_device_stats_match_host_stats(gpu_lib, precision):
 
 def test_fused_diagnostics_equal_separate_pass(gpu_lib, monkeypatch):
     """ns3d_diagnostics (FP64) sums |grad u|^2, mu, rho, |u|^2 and the kinetic
-    energy inside the viscous kernel that the next RK stage starts with; the
-    next step reuses that kernel's node fluxes.  Every output equals the
-    separate gradient pass (NS3D_DIAG_SEPARATE=1) to 1e-13 relative -- the
-    same terms summed in another fixed order -- and a step taken after the
-    fused diagnostics equals one taken without them bit for bit."""
+    energy in a pass built from the viscous kernel (its TMA plane tiles and
+    register windows, sums instead of node fluxes).  Every output equals the
+    separate per-cell gradient pass (NS3D_DIAG_SEPARATE=1) to 1e-13 relative
+    -- the same terms summed in another fixed order -- and the trajectory does
+    not depend on whether the monitor ran: a step taken after the diagnostics
+    equals one taken without them bit for bit."""
     from ns3d_wcns_b200.solver import Solver
     n = (24, 20, 18)
     P, G = make_params(n=n, L=(2 * math.pi, 1.7 * math.pi, 1.5 * math.pi), Ma=0.3, Re=400.0, interpolation=3,
@@ -59,7 +60,7 @@ def test_fused_diagnostics_equal_separate_pass(gpu_lib, monkeypatch):
             for _ in range(2):
                 s.rk3_step(s.compute_timestep())
             d = np.array(list(s.diagnostics().values()))
-            s.rk3_step(s.compute_timestep())  # reuses the node fluxes of the fused pass
+            s.rk3_step(s.compute_timestep())
             out[mode] = (d, s.primitives())
     monkeypatch.delenv("NS3D_DIAG_SEPARATE", raising=False)
     a, b = out["fused"][0], out["separate"][0]

@@ -235,9 +235,11 @@ def test_device_initialisers(gpu_lib, kind, bcs):
         assert per_var(W, Wr) <= 1e-15 and per_var(U, Ur) <= 1e-15
     else:
         assert np.array_equal(W, Wr) and np.array_equal(U, Ur)
-    # and the state then steps like the reference's
+    # and the state then steps like the reference's (relative to the largest
+    # conserved value: w, and v for sod / sine_x, stay zero up to rounding)
     ref.rk3_step(1e-4)
     with solver(P, G) as s:
         s.initialize(kind)
         s.rk3_step(1e-4)
-        assert per_var(s.conserved(), ref.conserved()) <= STEP_TOL
+        U, Ur = s.conserved(), ref.conserved()
+        assert np.abs(U - Ur).max() <= STEP_TOL * np.abs(Ur).max()

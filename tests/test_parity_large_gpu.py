@@ -12,7 +12,13 @@ instantiations and tilings the 256^3 benchmark runs:
     three y/z bundles (the last partial), nine y-chunks and six z-chunks,
     two z-segments of the viscous kernel.
 Tolerances (relative L-infinity over every cell, ghosts included, per
-variable): 1e-12 for one RHS, 1e-10 after 10 RK3 steps.  The time step of
+variable): 1e-12 for one RHS, 1e-10 after 10 RK3 steps.  The solenoidal
+isotropic field makes the continuity and energy right-hand sides small
+against the fluxes they are differences of (max |RHS_rho| = 0.2 at 64^3
+against momentum fluxes of ~10), so their rounding floor lies above 1e-12:
+perturbing the oracle's own inputs by +-1 ulp moves RHS_rho by ~3e-11 of
+its maximum.  Each variable's RHS bound is therefore max(1e-12, 4 x that
+measured 1-ulp sensitivity), computed in the test.  The time step of
 each step is the oracle's; the GPU's own compute_timestep must agree with
 it bit for bit at step 0 (identical state) and to 1e-13 relative after that
 (the states then differ by rounding: the RHS sums in another order).
@@ -91,14 +97,23 @@ def _detector_flips(U):
 def _run_pair(P, G, st, steps, count_detector=False):
     from ns3d_wcns_b200.solver import Solver
     o = _oracle(P, G)
+    # the rounding floor of each RHS variable: its change under +-1-ulp input perturbations
+    rng = np.random.default_rng(0)
+    o.set_interior_prims(*[f * (1 + rng.choice([-1.0, 0.0, 1.0], f.shape) * np.finfo(float).eps) for f in st])
+    o.compute_rhs()
+    R_pert = interior(o.rhs()).copy()
     o.set_interior_prims(*st)
     o.compute_rhs()
+    R_ref = interior(o.rhs()).copy()
+    sens = [rel_linf(a, b) for a, b in zip(R_pert, R_ref)]
     flips = near = 0
     with Solver(P, G) as s:
         s.set_interior_primitives(*st)
         s.compute_rhs()
-        rhs_err = _per_var(interior(s.rhs()), interior(o.rhs()))
-        assert rhs_err <= RHS_TOL, rhs_err
+        errs = [rel_linf(a, b) for a, b in zip(interior(s.rhs()), R_ref)]
+        rhs_err = max(errs)
+        for q in range(5):
+            assert errs[q] <= max(RHS_TOL, 4 * sens[q]), (q, errs, sens)
         dt_exact = 0
         for it in range(steps):
             if count_detector:
@@ -119,7 +134,8 @@ def _run_pair(P, G, st, steps, count_detector=False):
         prim_err = _per_var(s.primitives(), np.stack([o.get(k) for k in ("rho", "u", "v", "w", "p")]))
         ke_s, ke_o = s.total_energy(), o.total_energy()
     print(f"{G.global_nx}x{G.global_ny}x{G.global_nz} interp {P.interpolation} riemann {P.riemann_solver} "
-          f"char {P.char_recon}: rhs {rhs_err:.2e}, {steps} steps {step_err:.2e} (prims {prim_err:.2e}), "
+          f"char {P.char_recon}: rhs {[f'{e:.1e}' for e in errs]} (1-ulp floor {[f'{e:.1e}' for e in sens]}), "
+          f"{steps} steps {step_err:.2e} (prims {prim_err:.2e}), "
           f"dt bit-equal {dt_exact}/{steps}, detector flips {flips} near {near}")
     assert step_err <= STEP_TOL, step_err
     assert prim_err <= STEP_TOL, prim_err
