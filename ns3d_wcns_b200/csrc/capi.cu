@@ -482,6 +482,11 @@ ViscArgs<R> visc_args(ns3d_handle *h) {
     // the owned planes and the three either side whose fluxes the z-divergence reads
     a.zlo = h->zlo > 0 ? h->zlo - 3 : 0;
     a.zhi = h->zhi < a.L.nz ? h->zhi + 3 : a.L.nz;
+    // a slab with halos on both z sides is part of a z-periodic domain: over
+    // the planes it computes (three or more from its ends) every z derivative
+    // is the 6th-order one, as in that domain, and the kernel instantiation is
+    // the same one the whole periodic domain uses (same bits)
+    if (h->zlo > 0 && h->zhi < a.L.nz) a.periodic[2] = 1;
     a.red = nullptr;
     a.rlo = h->zlo; a.rhi = h->zhi;
     a.vol = h->ph.dx * h->ph.dy * h->ph.dz;
