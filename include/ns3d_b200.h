@@ -247,10 +247,15 @@ int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int check
  * time step.  No counterpart in the reference (one problem per process).
  * Plain FP64, inviscid (Re = inf), y and z periodic, any x boundary types,
  * component-wise interpolation.  Thread-block clusters take problems from an
- * atomic work queue, largest first; ns3d_batch_autotune times the cluster
- * size (1,2,4,8) x CTA width (128,256) x resident CTAs per SM (1,2,3: the
- * register budget of the kernel instantiation) choices and keeps the
- * fastest; config_out = {cluster, width, CTAs per SM}. */
+ * atomic work queue, largest first (the persistent schedule).  The
+ * wavefront schedule (cluster 0) instead advances every active problem one
+ * step per round of flat launches over all their cells, so uneven sizes
+ * keep the whole GPU busy; the host drops finished problems every 16 steps.
+ * Both give the same bits.  ns3d_batch_autotune times the wavefront and the
+ * persistent cluster size (1,2,4,8) x CTA width (128,256) x resident CTAs
+ * per SM (1,2,3: the register budget of the kernel instantiation) choices
+ * and keeps the fastest; config_out = {cluster (0: wavefront), width, CTAs
+ * per SM}. */
 typedef struct ns3d_batch ns3d_batch;
 int ns3d_batch_create(const ns3d_params *params, int n_problems, const ns3d_grid *grids, const double *t_end,
                       ns3d_batch **out);
@@ -318,7 +323,8 @@ int ns3d_debug_wait_timeout(int device, unsigned polls, int *code_out);
  * more, and six halo planes on each bordering side; the local z boundary
  * types must be non-periodic -- their treatment stays inside the halo) and,
  * when dz > 0, the global grid spacing (so the local dz is the global one bit
- * for bit).  The x/y sweeps then run over the owned planes, the viscous
+ * for bit); z_periodic = 1 when the whole domain is periodic in z (both of
+ * the slab's z sides are then halos).  The x/y sweeps then run over the owned planes, the viscous
  * fluxes over the owned planes and three halo planes each side, the z-sweep
  * updates owned cells only, and every reduction (time step, kinetic energy,
  * diagnostics) counts owned cells only.  ns3d_rk3_step / _steps /
@@ -329,7 +335,7 @@ int ns3d_debug_wait_timeout(int device, unsigned polls, int *code_out);
  * result are then exchanged through the pointers of ns3d_device_fields
  * (NS3D_PRIMITIVE and NS3D_TEMPERATURE), as runge_kutta_3's apply_boundary
  * does after every stage (range_kutta.cpp:61-63). */
-int ns3d_set_slab(ns3d_handle *h, int z_begin, int z_end, double dz);
+int ns3d_set_slab(ns3d_handle *h, int z_begin, int z_end, double dz, int z_periodic);
 int ns3d_rk3_stage(ns3d_handle *h, int stage, double dt);
 
 /* ---------------------------------------- scratch-free CFL time step

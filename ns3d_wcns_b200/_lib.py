@@ -91,7 +91,7 @@ def load() -> C.CDLL:
     lib.ns3d_time_advance.argtypes = [h, C.c_double, C.c_int, dp, C.POINTER(C.c_int)]
     lib.ns3d_device_fields.argtypes = [h, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_long)]
     lib.ns3d_set_stream.argtypes = [h, C.c_void_p]
-    lib.ns3d_set_slab.argtypes = [h, C.c_int, C.c_int, C.c_double]
+    lib.ns3d_set_slab.argtypes = [h, C.c_int, C.c_int, C.c_double, C.c_int]
     lib.ns3d_rk3_stage.argtypes = [h, C.c_int, C.c_double]
     lib.ns3d_synchronize.argtypes = [h]
     lib.ns3d_last_launch_count.argtypes = [h, C.POINTER(C.c_long)]

@@ -80,7 +80,8 @@ __device__ __forceinline__ void face_flux(const BatchArgs &a, const Inst &I, con
                                           int t2, double F[5]) {
     const Layout &L = I.L;
     const int n = DIR == 0 ? L.nx : (DIR == 1 ? L.ny : L.nz);
-    double st[5][6];
+    long id[6];
+#pragma unroll
     for (int m = 0; m < 6; ++m) {
         // ghost-inclusive cell along DIR: face g sits between cells (g-1+NG) and (g+NG) for x;
         // periodic directions: between g+NG and g+1+NG, stencil wrapped into [0, n+6)
@@ -90,11 +91,18 @@ __device__ __forceinline__ void face_flux(const BatchArgs &a, const Inst &I, con
             c = g + NG - 2 + m;
             if (c < NG) c += n; else if (c >= n + NG) c -= n;
         }
-        long id = DIR == 0 ? L.at(c, t1, t2) : (DIR == 1 ? L.at(t1, c, t2) : L.at(t1, t2, c));
-        for (int q = 0; q < 5; ++q) st[q][m] = Uc[(long)q * L.plane + id];
+        id[m] = DIR == 0 ? L.at(c, t1, t2) : (DIR == 1 ? L.at(t1, c, t2) : L.at(t1, t2, c));
     }
-    double wi[5] = {0, 0, 0, 0, 0};
-    wcns_face<DIR, double, INTERP, RS, 0>(a.sp, st, wi, wi, F);
+    // one variable's stencil at a time (WCNS_Riemann_InviscidFlux, component-wise)
+    double UL[5], UR[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        double f[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) f[m] = Uc[(long)q * L.plane + id[m]];
+        face_pair<double, INTERP>(a.sp, f, UL[q], UR[q]);
+    }
+    riemann<DIR, double, RS>(a.sp, UL, UR, F);
 }
 
 // INTERP / RS: compile-time scheme (RUNTIME: from a.sp); MINB: resident CTAs
@@ -283,6 +291,218 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(BatchArgs a) {
     }
 }
 
+// ------------------------------------------------- wavefront schedule
+//
+// Every active problem advances one step per sweep of a few flat launches:
+// each launch covers the cells of all stepping problems (a table maps block
+// b to a problem and a 256-cell tile of it), so the whole GPU works on every
+// phase however uneven the problem sizes are, and no problem's critical path
+// is bounded by the few CTAs of one cluster.  Each problem keeps its own
+// time, CFL time step, step count and status; the same face, update and
+// ghost-fill arithmetic as the persistent kernel, so the same bits.  Problems
+// that finish stop stepping and leave the tile tables when the host next
+// compacts them.
+struct WaveArgs {
+    const Inst *inst;
+    double *pool;
+    const int *tile_prob;        // block -> problem (sorted position)
+    const int *tile_off;         // block -> first cell of its tile
+    double cfl, gamma;
+    SchemeParams<double> sp;
+    unsigned long long *minbits; // per problem: bits of the CFL minimum (positive doubles order as integers)
+    double *t, *dt;              // per problem
+    int *steps, *status, *state_out, *stepping;
+    int max_steps;
+    int s0, stage;               // buffer holding the step-start state (same for all), stage 1..3
+};
+
+__device__ __forceinline__ double *warr(const WaveArgs &a, const Inst &I, int q) {
+    return a.pool + I.base + (long)q * I.L.plane;
+}
+
+// CFL minimum of each stepping problem over its interior cells (timestep.cpp:5-23)
+__global__ void __launch_bounds__(256) wave_cfl_kernel(WaveArgs a) {
+    const int p = a.tile_prob[blockIdx.x];
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const long e = (long)a.tile_off[blockIdx.x] + threadIdx.x;
+    double m = 1e9;
+    if (e < (long)L.nx * L.ny * L.nz) {
+        const int i = (int)(e % L.nx), jk = (int)(e / L.nx);
+        const long c = L.at(i + NG, jk % L.ny + NG, jk / L.ny + NG);
+        const double Us[5] = {warr(a, I, UOFF + 5 * a.s0)[c], warr(a, I, UOFF + 5 * a.s0 + 1)[c],
+                              warr(a, I, UOFF + 5 * a.s0 + 2)[c], warr(a, I, UOFF + 5 * a.s0 + 3)[c],
+                              warr(a, I, UOFF + 5 * a.s0 + 4)[c]};
+        m = cfl_bound(Us, a.gamma, I.dx);
+    }
+    __shared__ double mm;
+    block_min_n<256>(m, &mm);
+    // the bounds are positive (or the 1e9 cap), so their bit patterns order as the values
+    if (threadIdx.x == 0) atomicMin(&a.minbits[p], (unsigned long long)__double_as_longlong(mm));
+}
+
+// time_advance's schedule (maincycle.cpp:18-56) per problem, before a step
+__global__ void wave_schedule_kernel(WaveArgs a, int n) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    a.stepping[p] = 0;
+    if (a.status[p] != 2 || a.steps[p] >= a.max_steps) { a.minbits[p] = ~0ull; return; }  // done
+    const double t = a.t[p], t_end = a.inst[p].t_end;
+    const double m = __longlong_as_double((long long)a.minbits[p]);
+    a.minbits[p] = ~0ull;  // reset for the next step
+    if (fabs(t_end - t) <= 1e-12) { a.status[p] = 0; return; }
+    double dt = a.cfl * m;
+    if (t + dt > t_end) dt = t_end - t;
+    if (dt <= 1e-12) { a.status[p] = 1; return; }
+    a.t[p] = t + dt;
+    a.dt[p] = dt;
+    a.stepping[p] = 1;
+}
+
+// after a step: the count, the end test, and where the state is
+__global__ void wave_post_kernel(WaveArgs a, int n, int s_new) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n || !a.stepping[p]) return;
+    const int st = a.steps[p] + 1;
+    a.steps[p] = st;
+    a.state_out[p] = s_new;
+    if (a.t[p] >= a.inst[p].t_end) a.status[p] = 0;
+}
+
+// face fluxes of the stage's state: x-face g = i (and g = nx for the last
+// cell of a line), y-face j + 1/2, z-face k + 1/2 of interior cell (i, j, k)
+template <int INTERP, int RS>
+__global__ void __launch_bounds__(256) wave_face_kernel(WaveArgs a) {
+    const int p = a.tile_prob[blockIdx.x];
+    if (!a.stepping[p]) return;
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const long e = (long)a.tile_off[blockIdx.x] + threadIdx.x;
+    if (e >= (long)L.nx * L.ny * L.nz) return;
+    const int i = (int)(e % L.nx), jk = (int)(e / L.nx), j = jk % L.ny, k = jk / L.ny;
+    const int src = a.stage == 1 ? a.s0 : (a.stage == 2 ? (a.s0 + 1) % 3 : (a.s0 + 2) % 3);
+    const double *Uc = warr(a, I, UOFF + 5 * src);
+    BatchArgs b;
+    b.sp = a.sp;
+    b.gamma = a.gamma;
+    double F[5];
+    face_flux<0, INTERP, RS>(b, I, Uc, i, j + NG, k + NG, F);
+    long o = ((long)k * L.ny + j) * (L.nx + 1) + i;
+    for (int q = 0; q < 5; ++q) warr(a, I, 15 + q)[o] = F[q];
+    if (i == L.nx - 1) {
+        face_flux<0, INTERP, RS>(b, I, Uc, L.nx, j + NG, k + NG, F);
+        for (int q = 0; q < 5; ++q) warr(a, I, 15 + q)[o + 1] = F[q];
+    }
+    o = ((long)k * L.ny + j) * L.nx + i;
+    face_flux<1, INTERP, RS>(b, I, Uc, j, i + NG, k + NG, F);
+    for (int q = 0; q < 5; ++q) warr(a, I, 20 + q)[o] = F[q];
+    face_flux<2, INTERP, RS>(b, I, Uc, k, i + NG, j + NG, F);
+    for (int q = 0; q < 5; ++q) warr(a, I, 25 + q)[o] = F[q];
+}
+
+// RHS of interior cell (i, j, k) from the face fluxes, the stage update and
+// runge_kutta_3's c2p -> p2c round trip (range_kutta.cpp:53-91)
+__global__ void __launch_bounds__(256) wave_update_kernel(WaveArgs a) {
+    const int p = a.tile_prob[blockIdx.x];
+    if (!a.stepping[p]) return;
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const long e = (long)a.tile_off[blockIdx.x] + threadIdx.x;
+    if (e >= (long)L.nx * L.ny * L.nz) return;
+    const int i = (int)(e % L.nx), jk = (int)(e / L.nx), j = jk % L.ny, k = jk / L.ny;
+    const int stage = a.stage, s0 = a.s0;
+    const int src = stage == 1 ? s0 : (stage == 2 ? (s0 + 1) % 3 : (s0 + 2) % 3);
+    const int dst = stage == 2 ? (s0 + 2) % 3 : (s0 + 1) % 3;
+    const double dt = a.dt[p];
+    const long c = L.at(i + NG, j + NG, k + NG);
+    double Un[5], Wn[5], Ud[5];
+    for (int q = 0; q < 5; ++q) {
+        const double *FX = warr(a, I, 15 + q), *FY = warr(a, I, 20 + q), *FZ = warr(a, I, 25 + q);
+        auto fx = [&](int g) -> double {
+            if (g < 0) { if (I.bc[0] == BC_OUTFLOW) g = 0; else return 0.0; }
+            if (g > L.nx) { if (I.bc[1] == BC_OUTFLOW) g = L.nx; else return 0.0; }
+            return FX[((long)k * L.ny + j) * (L.nx + 1) + g];
+        };
+        auto dh = [](double f0, double f1, double f2, double f3, double f4, double f5, double ih) {
+            return ((f3 - f2) * (75.0 / 64.0) + (f4 - f1) * (-25.0 / 384.0) + (f5 - f0) * (3.0 / 640.0)) * ih;
+        };
+        double r = 0.0 - dh(fx(i - 2), fx(i - 1), fx(i), fx(i + 1), fx(i + 2), fx(i + 3), I.inv_dx);
+        auto fy = [&](int jj) {
+            jj = jj < 0 ? jj + L.ny : (jj >= L.ny ? jj - L.ny : jj);
+            return FY[((long)k * L.ny + jj) * L.nx + i];
+        };
+        auto fz = [&](int kk) {
+            kk = kk < 0 ? kk + L.nz : (kk >= L.nz ? kk - L.nz : kk);
+            return FZ[((long)kk * L.ny + j) * L.nx + i];
+        };
+        r = r - dh(fy(j - 3), fy(j - 2), fy(j - 1), fy(j), fy(j + 1), fy(j + 2), I.inv_dy);
+        r = r - dh(fz(k - 3), fz(k - 2), fz(k - 1), fz(k), fz(k + 1), fz(k + 2), I.inv_dz);
+        Un[q] = rk_combine(stage, warr(a, I, UOFF + 5 * s0 + q)[c], warr(a, I, UOFF + 5 * src + q)[c], r, dt);
+    }
+    c2p_exact(Un, a.gamma, Wn);
+    p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
+    for (int q = 0; q < 5; ++q) { warr(a, I, 5 * dst + q)[c] = Wn[q]; warr(a, I, UOFF + 5 * dst + q)[c] = Ud[q]; }
+}
+
+// ghost fill of the stage's new state (every non-interior cell of the box):
+// the persistent kernel's ghost phase
+__global__ void __launch_bounds__(256) wave_ghost_kernel(WaveArgs a) {
+    const int p = a.tile_prob[blockIdx.x];
+    if (!a.stepping[p]) return;
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const long e = (long)a.tile_off[blockIdx.x] + threadIdx.x;
+    if (e >= (long)L.sx * L.sy * L.sz) return;
+    int cc[3] = {(int)(e % L.sx), (int)((e / L.sx) % L.sy), (int)(e / ((long)L.sx * L.sy))};
+    if (is_interior(L, cc)) return;
+    const int ci = cc[0], cj = cc[1], ck = cc[2];
+    const int stage = a.stage, s0 = a.s0;
+    const int src = stage == 1 ? s0 : (stage == 2 ? (s0 + 1) % 3 : (s0 + 2) % 3);
+    const int dst = stage == 2 ? (s0 + 2) % 3 : (s0 + 1) % 3;
+    BcInfo b;
+    for (int d = 0; d < 3; ++d) b.periodic[d] = I.periodic[d];
+    for (int f = 0; f < 6; ++f) b.bc[f] = I.bc[f];
+    int flip;
+    const int kind = resolve_source(L, b, cc, flip);
+    double Wn[5];
+    if (kind != SRC_CELL) {
+        special_state(kind, Wn);
+    } else if (is_interior(L, cc)) {
+        const long s = L.at(cc[0], cc[1], cc[2]);
+        for (int q = 0; q < 5; ++q) Wn[q] = warr(a, I, 5 * dst + q)[s];
+    } else {
+        // a ghost cell no fill reaches keeps its own stage update with rhs = 0
+        const long s = L.at(cc[0], cc[1], cc[2]);
+        double Un[5];
+        for (int q = 0; q < 5; ++q)
+            Un[q] = rk_combine(stage, warr(a, I, UOFF + 5 * s0 + q)[s], warr(a, I, UOFF + 5 * src + q)[s], 0.0, a.dt[p]);
+        c2p_exact(Un, a.gamma, Wn);
+    }
+    apply_flips(flip, Wn);
+    const long o = L.at(ci, cj, ck);
+    double Ud[5];
+    p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
+    for (int q = 0; q < 5; ++q) { warr(a, I, 5 * dst + q)[o] = Wn[q]; warr(a, I, UOFF + 5 * dst + q)[o] = Ud[q]; }
+}
+
+// the conserved state of the initial buffer (every cell) and the per-problem
+// counters, before the first step
+__global__ void __launch_bounds__(256) wave_init_kernel(WaveArgs a) {
+    const int p = a.tile_prob[blockIdx.x];
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const long e = (long)a.tile_off[blockIdx.x] + threadIdx.x;
+    if (e == 0) {
+        a.t[p] = 0.0; a.steps[p] = 0; a.status[p] = 2; a.state_out[p] = 0; a.minbits[p] = ~0ull;
+        a.stepping[p] = 0;
+    }
+    if (e >= (long)L.sx * L.sy * L.sz) return;
+    const long o = L.at((int)(e % L.sx), (int)((e / L.sx) % L.sy), (int)(e / ((long)L.sx * L.sy)));
+    double Uo[5];
+    p2c_exact(warr(a, I, 0)[o], warr(a, I, 1)[o], warr(a, I, 2)[o], warr(a, I, 3)[o], warr(a, I, 4)[o], a.gamma, Uo);
+    for (int q = 0; q < 5; ++q) warr(a, I, UOFF + q)[o] = Uo[q];
+}
+
 __global__ void batch_scatter_interior(const double *src, double *dst, Layout L) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
     if (i >= L.nx) return;
@@ -326,7 +546,13 @@ struct ns3d_batch {
     double **d_tab = nullptr;    // scratch pointer table (10 pointers)
     cudaStream_t stream = nullptr;
     int device = 0;
-    int cluster = 4, threads = 256, minb = 1;
+    int cluster = 4, threads = 256, minb = 1;  // cluster 0: the wavefront schedule
+    // wavefront schedule: per-problem counters and the tile tables
+    void *wave = nullptr;
+    unsigned long long *w_minbits = nullptr;
+    double *w_dt = nullptr;
+    int *w_stepping = nullptr, *w_tiles = nullptr;  // tiles: [interior prob | interior off | box prob | box off]
+    long w_tile_cap = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_max_steps = -1;
     SchemeParams<double> sp;
@@ -394,6 +620,120 @@ int launch_batch(ns3d_batch *b, int max_steps, int cluster, int threads, int min
     cfg.gridDim = dim3(cluster * std::max(1, nclusters));
     BCK(b, cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream), "counter reset");
     BCK(b, cudaLaunchKernelEx(&cfg, kern, a), "batch launch");
+    return NS3D_OK;
+}
+
+WaveArgs wave_args(ns3d_batch *b, int max_steps) {
+    WaveArgs a;
+    a.inst = b->d_inst; a.pool = b->pool; a.cfl = b->P.cfl; a.gamma = b->P.gamma; a.sp = b->sp;
+    a.minbits = b->w_minbits; a.t = b->d_t; a.dt = b->w_dt; a.steps = b->d_steps; a.status = b->d_status;
+    a.state_out = b->d_state; a.stepping = b->w_stepping; a.max_steps = max_steps;
+    a.s0 = 0; a.stage = 0;
+    a.tile_prob = nullptr; a.tile_off = nullptr;
+    return a;
+}
+
+// Tile tables of the listed problems: 256 cells per block, interior cells
+// (faces, update, CFL) and whole boxes (ghost fill, initial conversion).
+int wave_tables(ns3d_batch *b, const std::vector<int> &probs, int &n_int, int &n_box) {
+    std::vector<int> ip, io, bp, bo;
+    for (int p : probs) {
+        const Layout &L = b->inst[p].L;
+        const long ni = (long)L.nx * L.ny * L.nz, nb = (long)L.sx * L.sy * L.sz;
+        for (long o = 0; o < ni; o += 256) { ip.push_back(p); io.push_back((int)o); }
+        for (long o = 0; o < nb; o += 256) { bp.push_back(p); bo.push_back((int)o); }
+    }
+    n_int = (int)ip.size();
+    n_box = (int)bp.size();
+    if ((long)(n_int + n_box) * 2 > b->w_tile_cap) return bfail(b, NS3D_ERR_STATE, "tile table capacity");
+    std::vector<int> all;
+    all.reserve(2 * (n_int + n_box));
+    all.insert(all.end(), ip.begin(), ip.end());
+    all.insert(all.end(), io.begin(), io.end());
+    all.insert(all.end(), bp.begin(), bp.end());
+    all.insert(all.end(), bo.begin(), bo.end());
+    if (!all.empty())
+        BCK(b, cudaMemcpyAsync(b->w_tiles, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream),
+            "tile tables");
+    BCK(b, cudaStreamSynchronize(b->stream), "synchronize");  // the host vector goes out of scope
+    return NS3D_OK;
+}
+
+int ensure_wave(ns3d_batch *b) {
+    if (b->wave) return NS3D_OK;
+    long tiles = 0;
+    for (const Inst &I : b->inst) {
+        const Layout &L = I.L;
+        tiles += ((long)L.nx * L.ny * L.nz + 255) / 256 + ((long)L.sx * L.sy * L.sz + 255) / 256;
+    }
+    b->w_tile_cap = 2 * tiles;
+    const size_t n = (size_t)b->n;
+    const size_t bytes = n * 8 + n * 8 + n * 4 + (size_t)b->w_tile_cap * 4 + 4 * 256;
+    BCK(b, cudaMalloc(&b->wave, bytes), "wavefront tables");
+    char *p = (char *)b->wave;
+    b->w_minbits = (unsigned long long *)p; p += (n * 8 + 255) / 256 * 256;
+    b->w_dt = (double *)p; p += (n * 8 + 255) / 256 * 256;
+    b->w_stepping = (int *)p; p += (n * 4 + 255) / 256 * 256;
+    b->w_tiles = (int *)p;
+    return NS3D_OK;
+}
+
+// The wavefront schedule to every problem's t_end (or max_steps): one step of
+// every active problem per round of launches; every 16 steps the host reads
+// the statuses and drops the finished problems from the tile tables.
+int run_wave(ns3d_batch *b, int max_steps) {
+    int r = ensure_wave(b);
+    if (r) return r;
+    WaveArgs a = wave_args(b, max_steps);
+    std::vector<int> active(b->n);
+    for (int p = 0; p < b->n; ++p) active[p] = p;
+    int n_int = 0, n_box = 0;
+    if ((r = wave_tables(b, active, n_int, n_box))) return r;
+    auto set_tables = [&](bool box) {
+        a.tile_prob = b->w_tiles + (box ? 2 * n_int : 0);
+        a.tile_off = b->w_tiles + (box ? 2 * n_int + n_box : n_int);
+    };
+    set_tables(true);
+    wave_init_kernel<<<n_box, 256, 0, b->stream>>>(a);
+    BCK(b, cudaGetLastError(), "wavefront init");
+    const unsigned pblocks = (unsigned)((b->n + 127) / 128);
+    const bool weno_roe = b->sp.interp == I_WENO5 && b->sp.riemann == R_ROE;
+    std::vector<int> status(b->n), steps(b->n);
+    int s0 = 0;
+    for (int step = 0; step < max_steps; ++step) {
+        if (step > 0 && step % 16 == 0) {
+            BCK(b, cudaMemcpyAsync(status.data(), b->d_status, sizeof(int) * b->n, cudaMemcpyDeviceToHost, b->stream),
+                "statuses");
+            BCK(b, cudaMemcpyAsync(steps.data(), b->d_steps, sizeof(int) * b->n, cudaMemcpyDeviceToHost, b->stream),
+                "steps");
+            BCK(b, cudaStreamSynchronize(b->stream), "synchronize");
+            std::vector<int> act;
+            for (int p : active)
+                if (status[p] == 2 && steps[p] < max_steps) act.push_back(p);
+            if (act.empty()) break;
+            if (act.size() != active.size()) {
+                active.swap(act);
+                if ((r = wave_tables(b, active, n_int, n_box))) return r;
+            }
+        }
+        a.s0 = s0;
+        set_tables(false);
+        wave_cfl_kernel<<<n_int, 256, 0, b->stream>>>(a);
+        wave_schedule_kernel<<<pblocks, 128, 0, b->stream>>>(a, b->n);
+        for (int stage = 1; stage <= 3; ++stage) {
+            a.stage = stage;
+            set_tables(false);
+            if (weno_roe) wave_face_kernel<I_WENO5, R_ROE><<<n_int, 256, 0, b->stream>>>(a);
+            else wave_face_kernel<RUNTIME, RUNTIME><<<n_int, 256, 0, b->stream>>>(a);
+            wave_update_kernel<<<n_int, 256, 0, b->stream>>>(a);
+            set_tables(true);
+            wave_ghost_kernel<<<n_box, 256, 0, b->stream>>>(a);
+        }
+        s0 = (s0 + 1) % 3;
+        wave_post_kernel<<<pblocks, 128, 0, b->stream>>>(a, b->n, s0);
+        BCK(b, cudaGetLastError(), "wavefront step");
+    }
+    BCK(b, cudaStreamSynchronize(b->stream), "synchronize");
     return NS3D_OK;
 }
 
@@ -501,6 +841,7 @@ int ns3d_batch_destroy(ns3d_batch *b) {
     if (b->stream) { cudaStreamSynchronize(b->stream); cudaStreamDestroy(b->stream); }
     if (b->pool) cudaFree(b->pool);
     if (b->meta) cudaFree(b->meta);
+    if (b->wave) cudaFree(b->wave);
     delete b;
     return NS3D_OK;
 }
@@ -534,6 +875,7 @@ int ns3d_batch_set_interior_primitives(ns3d_batch *b, int problem, const double 
 int ns3d_batch_run(ns3d_batch *b, int max_steps) {
     if (!b || max_steps < 1) return NS3D_ERR_INVALID_ARG;
     cudaSetDevice(b->device);
+    if (b->cluster == 0) return run_wave(b, max_steps);
     if (!b->graph || b->graph_max_steps != max_steps) {
         if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
         cudaGraph_t g;
@@ -562,25 +904,31 @@ int ns3d_batch_autotune(ns3d_batch *b, int trial_steps, int out[2]) {
     BCK(b, cudaMalloc(&save, b->pool_bytes), "autotune save buffer");
     cudaError_t se = cudaMemcpyAsync(save, b->pool, b->pool_bytes, cudaMemcpyDeviceToDevice, b->stream);
     if (se != cudaSuccess) { cudaFree(save); return bfail(b, NS3D_ERR_CUDA, "autotune save"); }
-    const int clusters[4] = {1, 2, 4, 8}, widths[2] = {128, 256}, minbs[3] = {1, 2, 3};
+    // cluster 0: the wavefront schedule (one configuration)
+    const int clusters[5] = {0, 1, 2, 4, 8}, widths[2] = {128, 256}, minbs[3] = {1, 2, 3};
     float best = 1e30f;
     int bc = b->cluster, bw = b->threads, bm = b->minb;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0); cudaEventCreate(&e1);
-    for (int ci = 0; ci < 4; ++ci)
+    for (int ci = 0; ci < 5; ++ci)
         for (int wi = 0; wi < 2; ++wi)
             for (int mi = 0; mi < 3; ++mi) {
+                if (clusters[ci] == 0 && (wi || mi)) continue;
                 if (cudaMemcpyAsync(b->pool, save, b->pool_bytes, cudaMemcpyDeviceToDevice, b->stream) != cudaSuccess) {
                     cudaGetLastError();
                     continue;
                 }
                 cudaEventRecord(e0, b->stream);
-                int r = launch_batch(b, trial_steps, clusters[ci], widths[wi], minbs[mi]);
+                int r = clusters[ci] == 0 ? run_wave(b, trial_steps)
+                                          : launch_batch(b, trial_steps, clusters[ci], widths[wi], minbs[mi]);
                 cudaEventRecord(e1, b->stream);
                 if (r || cudaStreamSynchronize(b->stream) != cudaSuccess) { cudaGetLastError(); continue; }
                 float ms = 0.f;
                 cudaEventElapsedTime(&ms, e0, e1);
-                if (ms < best) { best = ms; bc = clusters[ci]; bw = widths[wi]; bm = minbs[mi]; }
+                if (ms < best) {
+                    best = ms;
+                    bc = clusters[ci]; bw = clusters[ci] ? widths[wi] : 256; bm = clusters[ci] ? minbs[mi] : 1;
+                }
             }
     cudaEventDestroy(e0); cudaEventDestroy(e1);
     se = cudaMemcpyAsync(b->pool, save, b->pool_bytes, cudaMemcpyDeviceToDevice, b->stream);
@@ -594,8 +942,8 @@ int ns3d_batch_autotune(ns3d_batch *b, int trial_steps, int out[2]) {
 }
 
 int ns3d_batch_set_config(ns3d_batch *b, int cluster, int threads, int ctas_per_sm) {
-    if (!b || (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8) || (threads != 128 && threads != 256) ||
-        ctas_per_sm < 1 || ctas_per_sm > 3)
+    if (!b || (cluster != 0 && cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8) ||
+        (threads != 128 && threads != 256) || ctas_per_sm < 1 || ctas_per_sm > 3)
         return NS3D_ERR_INVALID_ARG;
     b->cluster = cluster; b->threads = threads; b->minb = ctas_per_sm;
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }

@@ -320,6 +320,7 @@ struct ns3d_handle {
     double *visc_red = nullptr;   // per-block diagnostics sums of the viscous kernel (5 per block)
     long visc_nblocks = 0;
     int step_start = -1;          // ns3d_rk3_stage: buffer the current step started from
+    bool slab_z_periodic = false; // a z-slab of a domain periodic in z
     double *scalars = nullptr;
     int red_blocks = 0;
     bool has_state = false;
@@ -482,11 +483,12 @@ ViscArgs<R> visc_args(ns3d_handle *h) {
     // the owned planes and the three either side whose fluxes the z-divergence reads
     a.zlo = h->zlo > 0 ? h->zlo - 3 : 0;
     a.zhi = h->zhi < a.L.nz ? h->zhi + 3 : a.L.nz;
-    // a slab with halos on both z sides is part of a z-periodic domain: over
-    // the planes it computes (three or more from its ends) every z derivative
-    // is the 6th-order one, as in that domain, and the kernel instantiation is
-    // the same one the whole periodic domain uses (same bits)
-    if (h->zlo > 0 && h->zhi < a.L.nz) a.periodic[2] = 1;
+    // a slab of a z-periodic domain: over the planes it computes (three or
+    // more from its ends) every z derivative is the 6th-order one, as in that
+    // domain, and the kernel instantiation is the one the whole periodic
+    // domain uses (same bits); a slab of a bounded domain keeps its local
+    // non-periodic instantiation, as the bounded domain does
+    if (h->slab_z_periodic) a.periodic[2] = 1;
     a.red = nullptr;
     a.rlo = h->zlo; a.rhi = h->zhi;
     a.vol = h->ph.dx * h->ph.dy * h->ph.dz;
@@ -1758,8 +1760,10 @@ int ns3d_time_advance(ns3d_handle *h, double t_end, int max_steps, double *time,
     return r;
 }
 
-int ns3d_set_slab(ns3d_handle *h, int z_begin, int z_end, double dz) {
+int ns3d_set_slab(ns3d_handle *h, int z_begin, int z_end, double dz, int z_periodic) {
     if (!h || z_begin < 0 || z_end > h->G.nz || z_end - z_begin < 1) return NS3D_ERR_INVALID_ARG;
+    if (z_periodic && (z_begin == 0 || z_end == h->G.nz))
+        return fail(h, NS3D_ERR_INVALID_ARG, "a slab of a z-periodic domain has halos on both z sides");
     if (!(dz > 0.0) && dz != 0.0) return NS3D_ERR_INVALID_ARG;
     const bool slab = z_begin != 0 || z_end != h->G.nz;
     if (slab && ((z_begin != 0 && z_begin < 6) || (z_end != h->G.nz && h->G.nz - z_end < 6) || z_end - z_begin < 6))
@@ -1774,6 +1778,7 @@ int ns3d_set_slab(ns3d_handle *h, int z_begin, int z_end, double dz) {
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     h->zlo = z_begin;
     h->zhi = z_end;
+    h->slab_z_periodic = z_periodic != 0;
     h->visc_valid = false;
     if (dz > 0.0) { h->ph.dz = dz; h->ph.inv_dz = 1.0 / dz; }
     h->cfl_valid = false;

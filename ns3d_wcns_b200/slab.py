@@ -194,7 +194,7 @@ class SlabSolver:
         self.s.set_stream(self.stream.cuda_stream)
         if plan.world > 1:
             # the global spacing, bit for bit (Lz / nz of the local extent may round differently)
-            self.s._check(self.s.lib.ns3d_set_slab(self.s.h, plan.zlo, plan.zhi, float(G.dz)))
+            self.s._check(self.s.lib.ns3d_set_slab(self.s.h, plan.zlo, plan.zhi, float(G.dz), int(plan.periodic)))
         self._exchange = exchange_fn or (lambda pl, planes: exchange(pl, planes))
         self._min = allreduce_min or _dist_allreduce(min_op=True)
         self._sum = allreduce_sum or _dist_allreduce(min_op=False)

@@ -1,6 +1,7 @@
 """Batched persistent launch (ns3d_batch_*): every problem against the oracle
 running the reference's own dt schedule (maincycle.cpp:18-56) on that
-problem; results independent of the autotuned launch configuration."""
+problem; results independent of the autotuned launch configuration, the
+persistent cluster schedules and the wavefront schedule alike."""
 import math
 
 import numpy as np
@@ -55,12 +56,15 @@ def problems(interp=0, rs=0):
     return P, grids, states, t_end
 
 
+@pytest.mark.parametrize("schedule", ["persistent", "wavefront"])
 @pytest.mark.parametrize("scheme", [(0, 0), (3, 2)])
-def test_batch_matches_oracle_per_problem(gpu_lib, scheme):
+def test_batch_matches_oracle_per_problem(gpu_lib, scheme, schedule):
     P, grids, states, t_end = problems(*scheme)
     with Batch(P, grids, t_end) as b:
         for i, st in enumerate(states):
             b.set_interior_primitives(i, *st)
+        if schedule == "wavefront":
+            b.set_config(0, 256, 1)
         b.run()
         for i, (g, st) in enumerate(zip(grids, states)):
             W, t, steps = oracle_run(P, g, st, t_end[i])
@@ -73,7 +77,8 @@ def test_batch_matches_oracle_per_problem(gpu_lib, scheme):
 def test_batch_results_do_not_depend_on_launch_config(gpu_lib):
     P, grids, states, t_end = problems()
     outs = []
-    for cfg in [(1, 128, 1), (4, 256, 2), (8, 128, 3), (2, 256, 3)]:
+    # cluster 0: the wavefront schedule
+    for cfg in [(1, 128, 1), (4, 256, 2), (8, 128, 3), (2, 256, 3), (0, 256, 1)]:
         with Batch(P, grids, t_end) as b:
             for i, st in enumerate(states):
                 b.set_interior_primitives(i, *st)
@@ -91,7 +96,7 @@ def test_autotune_picks_a_valid_config_and_keeps_the_state(gpu_lib):
         for i, st in enumerate(states):
             b.set_interior_primitives(i, *st)
         cl, th, mb = b.autotune(trial_steps=5)
-        assert cl in (1, 2, 4, 8) and th in (128, 256) and mb in (1, 2, 3)
+        assert cl in (0, 1, 2, 4, 8) and th in (128, 256) and mb in (1, 2, 3)
         b.run()
         W, t, steps = oracle_run(P, grids[0], states[0], t_end[0])
         assert max(rel_linf(a, r) for a, r in zip(b.primitives(0), W)) <= 1e-10
