@@ -69,24 +69,39 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    PERIOD_MS = 50
+
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host arrival time, csv line)
+        self.t_begin = self.t_end = None
 
     def start(self):
+        """Start sampling and wait for the first sample, so that the timed
+        region that follows is covered from its start."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", str(self.PERIOD_MS), "-i", str(self.device)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t0 = time.monotonic()
+        while not self.lines and self.proc.poll() is None and time.monotonic() - t0 < 10:
+            time.sleep(0.01)
+
+    def begin(self):
+        self.t_begin = time.monotonic()
+
+    def end(self):
+        self.t_end = time.monotonic()
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def stop(self):
         if not self.proc:
@@ -99,7 +114,12 @@ class ClockSampler:
         self.t.join(timeout=2)
         sm, smax, reasons, power = [], [], set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # samples that arrived inside the timed region (plus one period for the read latency)
+        lo = self.t_begin if self.t_begin is not None else -math.inf
+        hi = self.t_end + self.PERIOD_MS * 1e-3 if self.t_end is not None else math.inf
+        for t, ln in self.lines:
+            if not lo <= t <= hi:
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -544,10 +564,12 @@ def run_slabs(args, rank, world, local, dist):
     clk.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sv.launch_count = 0
+    clk.begin()
     e0.record(stream)
     steps(args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
+    clk.end()
     ms = max_over_ranks(e0.elapsed_time(e1))
     clocks = clk.stop()
     launches = sv.launch_count
@@ -601,7 +623,7 @@ def run_slabs(args, rank, world, local, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
@@ -696,10 +718,12 @@ def main():
         clk = ClockSampler(local)
         clk.start()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clk.begin()
         e0.record(stream)
         t, done = s.time_advance(t_far, args.steps, t)
         e1.record(stream)
         torch.cuda.synchronize()
+        clk.end()
         ms = e0.elapsed_time(e1)
         clocks = clk.stop()
         launches = s.launches()

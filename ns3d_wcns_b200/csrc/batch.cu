@@ -456,6 +456,14 @@ __global__ void __launch_bounds__(256) wave_ghost_kernel(WaveArgs a) {
     int cc[3] = {(int)(e % L.sx), (int)((e / L.sx) % L.sy), (int)(e / ((long)L.sx * L.sy))};
     if (is_interior(L, cc)) return;
     const int ci = cc[0], cj = cc[1], ck = cc[2];
+    // Within a run only two kinds of ghost cell are read: the x ghosts of
+    // interior lines (by the x-face stencils) and the ghosts no fill reaches
+    // (by their own zero-RHS update).  The others -- copies of interior
+    // cells, constants -- are a function of the current state alone, so one
+    // fill at the end of the run (wave_final_fill_kernel) gives them the
+    // values the per-stage fill would have left.
+    const bool x_ghost_line = (ci < NG || ci >= L.nx + NG) && cj >= NG && cj < L.ny + NG && ck >= NG &&
+                              ck < L.nz + NG;
     const int stage = a.stage, s0 = a.s0;
     const int src = stage == 1 ? s0 : (stage == 2 ? (s0 + 1) % 3 : (s0 + 2) % 3);
     const int dst = stage == 2 ? (s0 + 2) % 3 : (s0 + 1) % 3;
@@ -464,10 +472,12 @@ __global__ void __launch_bounds__(256) wave_ghost_kernel(WaveArgs a) {
     for (int f = 0; f < 6; ++f) b.bc[f] = I.bc[f];
     int flip;
     const int kind = resolve_source(L, b, cc, flip);
+    const bool unreached = kind == SRC_CELL && !is_interior(L, cc);
+    if (!x_ghost_line && !unreached) return;
     double Wn[5];
     if (kind != SRC_CELL) {
         special_state(kind, Wn);
-    } else if (is_interior(L, cc)) {
+    } else if (!unreached) {
         const long s = L.at(cc[0], cc[1], cc[2]);
         for (int q = 0; q < 5; ++q) Wn[q] = warr(a, I, 5 * dst + q)[s];
     } else {
@@ -483,6 +493,38 @@ __global__ void __launch_bounds__(256) wave_ghost_kernel(WaveArgs a) {
     double Ud[5];
     p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
     for (int q = 0; q < 5; ++q) { warr(a, I, 5 * dst + q)[o] = Wn[q]; warr(a, I, UOFF + 5 * dst + q)[o] = Ud[q]; }
+}
+
+// The ghost cells the per-stage fill leaves out, once at the end of a run:
+// copies of (the final state's) interior cells with their sign flips, and
+// constants -- the values the last stage's fill would have given them.
+__global__ void __launch_bounds__(256) wave_final_fill_kernel(WaveArgs a) {
+    const int p = a.tile_prob[blockIdx.x];
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const long e = (long)a.tile_off[blockIdx.x] + threadIdx.x;
+    if (e >= (long)L.sx * L.sy * L.sz || a.steps[p] == 0) return;
+    int cc[3] = {(int)(e % L.sx), (int)((e / L.sx) % L.sy), (int)(e / ((long)L.sx * L.sy))};
+    if (is_interior(L, cc)) return;
+    const long o = L.at(cc[0], cc[1], cc[2]);
+    BcInfo b;
+    for (int d = 0; d < 3; ++d) b.periodic[d] = I.periodic[d];
+    for (int f = 0; f < 6; ++f) b.bc[f] = I.bc[f];
+    int flip;
+    const int kind = resolve_source(L, b, cc, flip);
+    if (kind == SRC_CELL && !is_interior(L, cc)) return;  // evolved by its own updates
+    const int buf = a.state_out[p];
+    double Wn[5];
+    if (kind != SRC_CELL) {
+        special_state(kind, Wn);
+    } else {
+        const long s = L.at(cc[0], cc[1], cc[2]);
+        for (int q = 0; q < 5; ++q) Wn[q] = warr(a, I, 5 * buf + q)[s];
+    }
+    apply_flips(flip, Wn);
+    double Ud[5];
+    p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
+    for (int q = 0; q < 5; ++q) { warr(a, I, 5 * buf + q)[o] = Wn[q]; warr(a, I, UOFF + 5 * buf + q)[o] = Ud[q]; }
 }
 
 // the conserved state of the initial buffer (every cell) and the per-problem
@@ -733,6 +775,13 @@ int run_wave(ns3d_batch *b, int max_steps) {
         wave_post_kernel<<<pblocks, 128, 0, b->stream>>>(a, b->n, s0);
         BCK(b, cudaGetLastError(), "wavefront step");
     }
+    // the ghost cells left out of the per-stage fills, every problem
+    std::vector<int> all(b->n);
+    for (int p = 0; p < b->n; ++p) all[p] = p;
+    if ((r = wave_tables(b, all, n_int, n_box))) return r;
+    set_tables(true);
+    wave_final_fill_kernel<<<n_box, 256, 0, b->stream>>>(a);
+    BCK(b, cudaGetLastError(), "final ghost fill");
     BCK(b, cudaStreamSynchronize(b->stream), "synchronize");
     return NS3D_OK;
 }
