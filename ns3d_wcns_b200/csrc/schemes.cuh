@@ -9,6 +9,8 @@
 // result is mathematically identical and differs only in rounding.
 #pragma once
 
+#include <cstring>
+
 #include "common.cuh"
 
 #ifndef NS3D_HD
@@ -100,11 +102,13 @@ NS3D_HD float mdcd_beta3(float f0, float f1, float f2, float f3, float f4, float
 //
 // The detector is the one discontinuous decision of the scheme, so the FP64
 // build takes the reference's decision exactly: the cross-multiplied test
-// (whose products the compiler may fuse) decides every case farther than
-// 1e-12 relative from the threshold -- far beyond its few-ulp rounding -- and
-// the rest are decided by the reference's own quotient, term by term with
-// unfused IEEE operations (mdcd_sai_ref).  a and b themselves round as in the
-// reference: 2 f is exact, so a fused f0 - 2 fm1 gives the same bits.
+// (whose products the compiler may fuse) decides every case whose two sides
+// lie at least two units apart in their high 32-bit words (more than 2^-21
+// relative, far beyond the test's few-ulp rounding; an integer test, so the
+// FP64 pipe does no extra work), and the rest are decided by the reference's
+// own quotient, term by term with unfused IEEE operations (mdcd_sai_ref).  a
+// and b themselves round as in the reference: 2 f is exact, so a fused
+// f0 - 2 fm1 gives the same bits.
 NS3D_HD double mdcd_sai_ref(double a, double b) {
     const double eps = 0.9 * 0.4 / (1.0 - 0.9 * 0.4) * 1e-4;
 #ifdef __CUDA_ARCH__
@@ -117,6 +121,17 @@ NS3D_HD double mdcd_sai_ref(double a, double b) {
 #endif
 }
 
+// high 32 bits of an FP64 value (sign, exponent, top 20 mantissa bits)
+NS3D_HD int f64_hi_word(double x) {
+#ifdef __CUDA_ARCH__
+    return __double2hiint(x);
+#else
+    unsigned long long u;
+    std::memcpy(&u, &x, sizeof u);
+    return (int)(u >> 32);
+#endif
+}
+
 template <typename R>
 NS3D_HD bool mdcd_smooth(R fm2, R fm1, R f0, R fp1, R fp2) {
     const R eps = R(0.9 * 0.4 / (1.0 - 0.9 * 0.4) * 1e-4);
@@ -124,8 +139,24 @@ NS3D_HD bool mdcd_smooth(R fm2, R fm1, R f0, R fp1, R fp2) {
     R b = fabs(f0 - fp1) + fabs(f0 - R(2) * fp1 + fp2);
     const R lhs = R(2) * a * b + eps, rhs = R(0.4) * (a * a + b * b + eps);
     if constexpr (sizeof(R) == 8) {
-        if (fabs(lhs - rhs) <= 1e-12 * rhs) return mdcd_sai_ref(a, b) > 0.4;
+        // lhs, rhs > 0, so their high words order as the values do
+        if ((unsigned)(f64_hi_word(lhs) - f64_hi_word(rhs) + 1) <= 2u) return mdcd_sai_ref(a, b) > 0.4;
     }
+    return lhs > rhs;
+}
+
+// The cross-multiplied decision alone, without a branch: near is set (FP64)
+// where the two sides are too close for it, and the caller then takes
+// mdcd_smooth's decision instead (once for all the detectors of a cell, so
+// the common path has no branch per detector).  Wherever near stays clear the
+// value equals mdcd_smooth's.
+template <typename R>
+NS3D_HD bool mdcd_smooth_fast(R fm2, R fm1, R f0, R fp1, R fp2, bool &near) {
+    const R eps = R(0.9 * 0.4 / (1.0 - 0.9 * 0.4) * 1e-4);
+    R a = fabs(f0 - fm1) + fabs(f0 - R(2) * fm1 + fm2);
+    R b = fabs(f0 - fp1) + fabs(f0 - R(2) * fp1 + fp2);
+    const R lhs = R(2) * a * b + eps, rhs = R(0.4) * (a * a + b * b + eps);
+    if constexpr (sizeof(R) == 8) near |= (unsigned)(f64_hi_word(lhs) - f64_hi_word(rhs) + 1) <= 2u;
     return lhs > rhs;
 }
 

@@ -197,6 +197,22 @@ __device__ __forceinline__ void fused_stage_cell(const FusedStage &f, double dt,
     }
 }
 
+// The detector bits of a cell (and of the line's first cell) again with
+// mdcd_smooth's exact decisions, for the rare cell where one of the
+// cross-multiplied tests was too close to call.  Stencils re-read from shared
+// memory, so no registers stay alive across the common path.
+template <typename R, int NL, int NU, typename G>
+__device__ __noinline__ uint2 detect_exact(const R *sU, int line, int slot, bool first) {
+    unsigned r3 = 0, r2f = 0;  // as in the sweep: bit q for cell f+1 / f
+    for (int q = 0; q < 5; ++q) {
+        R sq[6];
+        for (int m = 0; m < 6; ++m) sq[m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
+        r3 |= (mdcd_smooth(sq[1], sq[2], sq[3], sq[4], sq[5]) ? 0u : 1u) << q;
+        if (first) r2f |= (mdcd_smooth(sq[0], sq[1], sq[2], sq[3], sq[4]) ? 0u : 1u) << q;
+    }
+    return make_uint2(r3, r2f);
+}
+
 template <int DIR, typename R, int INTERP, int RS, int CHAR>
 __global__ void __launch_bounds__(256, sweep_min_blocks<DIR, R>())
 sweep_kernel(SweepArgs<R> a) {
@@ -376,16 +392,22 @@ sweep_kernel(SweepArgs<R> a) {
                 // the rare WENO branch re-reads its stencil from shared memory
                 R UL[5], UR[5];
                 unsigned r3 = 0, r2f = 0;  // bit q: the detector rejects the linear scheme at cell f+1 / f
+                bool near = false;
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
                     R sq[6];
 #pragma unroll
                     for (int m = 0; m < 6; ++m) sq[m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
-                    r3 |= (mdcd_smooth(sq[1], sq[2], sq[3], sq[4], sq[5]) ? 0u : 1u) << q;
+                    r3 |= (mdcd_smooth_fast(sq[1], sq[2], sq[3], sq[4], sq[5], near) ? 0u : 1u) << q;
                     if (fc == fb && slot == 0)
-                        r2f |= (mdcd_smooth(sq[0], sq[1], sq[2], sq[3], sq[4]) ? 0u : 1u) << q;
+                        r2f |= (mdcd_smooth_fast(sq[0], sq[1], sq[2], sq[3], sq[4], near) ? 0u : 1u) << q;
                     UL[q] = mdcd_linear(a.sp.lin, sq[0], sq[1], sq[2], sq[3], sq[4], sq[5]);
                     UR[q] = mdcd_linear(a.sp.lin, sq[5], sq[4], sq[3], sq[2], sq[1], sq[0]);
+                }
+                if (near) {
+                    const uint2 e = detect_exact<R, NL, NU, G>(sU, line, slot, fc == fb && slot == 0);
+                    r3 = e.x;
+                    r2f = e.y;
                 }
                 unsigned r2 = __shfl_up_sync(0xffffffffu, r3, 1);
                 if (slot == 0) r2 = fc == fb ? r2f : det_carry;
@@ -425,16 +447,22 @@ sweep_kernel(SweepArgs<R> a) {
             unsigned r3 = 0;
             if (act) {
                 unsigned r2f = 0;
+                bool near = false;
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
                     R sq[6];
 #pragma unroll
                     for (int m = 0; m < 6; ++m) sq[m] = sU[q * NL * NU + G::template idx<NU>(line, slot + m)];
-                    r3 |= (mdcd_smooth(sq[1], sq[2], sq[3], sq[4], sq[5]) ? 0u : 1u) << q;
+                    r3 |= (mdcd_smooth_fast(sq[1], sq[2], sq[3], sq[4], sq[5], near) ? 0u : 1u) << q;
                     if (fc == fb && slot == 0)
-                        r2f |= (mdcd_smooth(sq[0], sq[1], sq[2], sq[3], sq[4]) ? 0u : 1u) << q;
+                        r2f |= (mdcd_smooth_fast(sq[0], sq[1], sq[2], sq[3], sq[4], near) ? 0u : 1u) << q;
                     UL[q] = mdcd_linear(a.sp.lin, sq[0], sq[1], sq[2], sq[3], sq[4], sq[5]);
                     UR[q] = mdcd_linear(a.sp.lin, sq[5], sq[4], sq[3], sq[2], sq[1], sq[0]);
+                }
+                if (near) {
+                    const uint2 e = detect_exact<R, NL, NU, G>(sU, line, slot, fc == fb && slot == 0);
+                    r3 = e.x;
+                    r2f = e.y;
                 }
                 sDet[(slot + 1) * NL + line] = (unsigned char)r3;
                 if (fc == fb && slot == 0) sDet[line] = (unsigned char)r2f;
