@@ -314,7 +314,28 @@ struct WaveArgs {
     int *steps, *status, *state_out, *stepping;
     int max_steps;
     int s0, stage;               // buffer holding the step-start state (same for all), stage 1..3
+    // (problem, box cell) lists, wave_ghost_list_kernel: [0] the ghost cells a
+    // stage fills, [1] the ghost cells no fill reaches that are their own
+    // source, [2] those whose source is another such cell (kind 1)
+    const int2 *ghosts;
+    int n_ghost[3], ghost_base[3];
+    int *ghost_count;            // [3]: entries found (list building)
+    double *dt_hist;             // [WAVE_WINDOW][n]: dt of each step of the window, -1: did not step
+    int hist_slot, n_prob;
 };
+
+// Ghost cells no fill reaches evolve by their own zero-RHS stage updates and
+// are read by nothing else, so they are advanced in windows of WAVE_WINDOW
+// steps (wave_unreached_kernel, registers only) from the recorded dt values
+// instead of through memory at every stage.
+constexpr int WAVE_WINDOW = 16;
+
+// Problems whose cross-section has at most BRICK_COLS cells take the fused
+// face + update kernel (wave_brick_kernel) on bricks of 256 / (ny nz) x-cells
+// by the whole cross-section; larger cross-sections the separate kernels.
+constexpr int BRICK_COLS = 64;
+__host__ __device__ __forceinline__ bool brick_ok(const Layout &L) { return L.ny * L.nz <= BRICK_COLS; }
+__host__ __device__ __forceinline__ int brick_width(const Layout &L) { return 256 / (L.ny * L.nz); }
 
 __device__ __forceinline__ double *warr(const WaveArgs &a, const Inst &I, int q) {
     return a.pool + I.base + (long)q * I.L.plane;
@@ -346,6 +367,7 @@ __global__ void wave_schedule_kernel(WaveArgs a, int n) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     a.stepping[p] = 0;
+    a.dt_hist[(long)a.hist_slot * n + p] = -1.0;
     if (a.status[p] != 2 || a.steps[p] >= a.max_steps) { a.minbits[p] = ~0ull; return; }  // done
     const double t = a.t[p], t_end = a.inst[p].t_end;
     const double m = __longlong_as_double((long long)a.minbits[p]);
@@ -356,6 +378,7 @@ __global__ void wave_schedule_kernel(WaveArgs a, int n) {
     if (dt <= 1e-12) { a.status[p] = 1; return; }
     a.t[p] = t + dt;
     a.dt[p] = dt;
+    a.dt_hist[(long)a.hist_slot * n + p] = dt;
     a.stepping[p] = 1;
 }
 
@@ -377,6 +400,7 @@ __global__ void __launch_bounds__(256) wave_face_kernel(WaveArgs a) {
     if (!a.stepping[p]) return;
     const Inst &I = a.inst[p];
     const Layout &L = I.L;
+    if (brick_ok(L)) return;  // wave_brick_kernel's
     const long e = (long)a.tile_off[blockIdx.x] + threadIdx.x;
     if (e >= (long)L.nx * L.ny * L.nz) return;
     const int i = (int)(e % L.nx), jk = (int)(e / L.nx), j = jk % L.ny, k = jk / L.ny;
@@ -400,33 +424,64 @@ __global__ void __launch_bounds__(256) wave_face_kernel(WaveArgs a) {
     for (int q = 0; q < 5; ++q) warr(a, I, 25 + q)[o] = F[q];
 }
 
-// RHS of interior cell (i, j, k) from the face fluxes, the stage update and
-// runge_kutta_3's c2p -> p2c round trip (range_kutta.cpp:53-91)
+// RHS of one variable at interior cell (i, j, k) from its face fluxes: the
+// 6th-order half-node difference in x, then y, then z (fx: x-face g with the
+// boundary rule for g outside [0, nx]; fy / fz: periodic face index)
+template <class FX, class FY, class FZ>
+__device__ __forceinline__ double wave_rhs(const Inst &I, int i, int j, int k, FX fx, FY fy, FZ fz) {
+    auto dh = [](double f0, double f1, double f2, double f3, double f4, double f5, double ih) {
+        return ((f3 - f2) * (75.0 / 64.0) + (f4 - f1) * (-25.0 / 384.0) + (f5 - f0) * (3.0 / 640.0)) * ih;
+    };
+    double r = 0.0 - dh(fx(i - 2), fx(i - 1), fx(i), fx(i + 1), fx(i + 2), fx(i + 3), I.inv_dx);
+    r = r - dh(fy(j - 3), fy(j - 2), fy(j - 1), fy(j), fy(j + 1), fy(j + 2), I.inv_dy);
+    r = r - dh(fz(k - 3), fz(k - 2), fz(k - 1), fz(k), fz(k + 1), fz(k + 2), I.inv_dz);
+    return r;
+}
+
+// x-face index with the boundary rule: faces beyond the domain take the
+// boundary face's flux at an outflow side, zero otherwise (-1)
+__device__ __forceinline__ int wave_xface(const Inst &I, int g) {
+    if (g < 0) return I.bc[0] == BC_OUTFLOW ? 0 : -1;
+    if (g > I.L.nx) return I.bc[1] == BC_OUTFLOW ? I.L.nx : -1;
+    return g;
+}
+
+// the stage update of interior cell c from its RHS and runge_kutta_3's
+// c2p -> p2c round trip (range_kutta.cpp:53-91)
+__device__ __forceinline__ void wave_finish(const WaveArgs &a, const Inst &I, long c, int dst, int src,
+                                            const double r[5], double dt) {
+    double Un[5], Wn[5], Ud[5];
+    for (int q = 0; q < 5; ++q)
+        Un[q] = rk_combine(a.stage, warr(a, I, UOFF + 5 * a.s0 + q)[c], warr(a, I, UOFF + 5 * src + q)[c], r[q], dt);
+    c2p_exact(Un, a.gamma, Wn);
+    p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
+    for (int q = 0; q < 5; ++q) { warr(a, I, 5 * dst + q)[c] = Wn[q]; warr(a, I, UOFF + 5 * dst + q)[c] = Ud[q]; }
+}
+
+__device__ __forceinline__ int wave_src(const WaveArgs &a) {
+    return a.stage == 1 ? a.s0 : (a.stage == 2 ? (a.s0 + 1) % 3 : (a.s0 + 2) % 3);
+}
+__device__ __forceinline__ int wave_dst(const WaveArgs &a) {
+    return a.stage == 2 ? (a.s0 + 2) % 3 : (a.s0 + 1) % 3;
+}
+
+// RHS of interior cell (i, j, k) from the face fluxes and the stage update
 __global__ void __launch_bounds__(256) wave_update_kernel(WaveArgs a) {
     const int p = a.tile_prob[blockIdx.x];
     if (!a.stepping[p]) return;
     const Inst &I = a.inst[p];
     const Layout &L = I.L;
+    if (brick_ok(L)) return;  // wave_brick_kernel's
     const long e = (long)a.tile_off[blockIdx.x] + threadIdx.x;
     if (e >= (long)L.nx * L.ny * L.nz) return;
     const int i = (int)(e % L.nx), jk = (int)(e / L.nx), j = jk % L.ny, k = jk / L.ny;
-    const int stage = a.stage, s0 = a.s0;
-    const int src = stage == 1 ? s0 : (stage == 2 ? (s0 + 1) % 3 : (s0 + 2) % 3);
-    const int dst = stage == 2 ? (s0 + 2) % 3 : (s0 + 1) % 3;
-    const double dt = a.dt[p];
-    const long c = L.at(i + NG, j + NG, k + NG);
-    double Un[5], Wn[5], Ud[5];
+    double r[5];
     for (int q = 0; q < 5; ++q) {
         const double *FX = warr(a, I, 15 + q), *FY = warr(a, I, 20 + q), *FZ = warr(a, I, 25 + q);
         auto fx = [&](int g) -> double {
-            if (g < 0) { if (I.bc[0] == BC_OUTFLOW) g = 0; else return 0.0; }
-            if (g > L.nx) { if (I.bc[1] == BC_OUTFLOW) g = L.nx; else return 0.0; }
-            return FX[((long)k * L.ny + j) * (L.nx + 1) + g];
+            g = wave_xface(I, g);
+            return g < 0 ? 0.0 : FX[((long)k * L.ny + j) * (L.nx + 1) + g];
         };
-        auto dh = [](double f0, double f1, double f2, double f3, double f4, double f5, double ih) {
-            return ((f3 - f2) * (75.0 / 64.0) + (f4 - f1) * (-25.0 / 384.0) + (f5 - f0) * (3.0 / 640.0)) * ih;
-        };
-        double r = 0.0 - dh(fx(i - 2), fx(i - 1), fx(i), fx(i + 1), fx(i + 2), fx(i + 3), I.inv_dx);
         auto fy = [&](int jj) {
             jj = jj < 0 ? jj + L.ny : (jj >= L.ny ? jj - L.ny : jj);
             return FY[((long)k * L.ny + jj) * L.nx + i];
@@ -435,64 +490,201 @@ __global__ void __launch_bounds__(256) wave_update_kernel(WaveArgs a) {
             kk = kk < 0 ? kk + L.nz : (kk >= L.nz ? kk - L.nz : kk);
             return FZ[((long)kk * L.ny + j) * L.nx + i];
         };
-        r = r - dh(fy(j - 3), fy(j - 2), fy(j - 1), fy(j), fy(j + 1), fy(j + 2), I.inv_dy);
-        r = r - dh(fz(k - 3), fz(k - 2), fz(k - 1), fz(k), fz(k + 1), fz(k + 2), I.inv_dz);
-        Un[q] = rk_combine(stage, warr(a, I, UOFF + 5 * s0 + q)[c], warr(a, I, UOFF + 5 * src + q)[c], r, dt);
+        r[q] = wave_rhs(I, i, j, k, fx, fy, fz);
     }
-    c2p_exact(Un, a.gamma, Wn);
-    p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
-    for (int q = 0; q < 5; ++q) { warr(a, I, 5 * dst + q)[c] = Wn[q]; warr(a, I, UOFF + 5 * dst + q)[c] = Ud[q]; }
+    wave_finish(a, I, L.at(i + NG, j + NG, k + NG), wave_dst(a), wave_src(a), r, a.dt[p]);
 }
 
-// ghost fill of the stage's new state (every non-interior cell of the box):
-// the persistent kernel's ghost phase
-__global__ void __launch_bounds__(256) wave_ghost_kernel(WaveArgs a) {
+// Faces and update of one brick -- bx x-cells by the whole ny x nz
+// cross-section of one problem -- in one kernel: the brick's x-faces (with
+// the 2 + 3 faces beyond its ends the difference stencil needs), y-faces and
+// z-faces go to shared memory, then each thread updates one cell from them.
+// The same face_flux and update arithmetic as wave_face_kernel +
+// wave_update_kernel, so the same bits, without the global face arrays'
+// round trip and one launch per stage fewer.
+template <int INTERP, int RS>
+__global__ void __launch_bounds__(256) wave_brick_kernel(WaveArgs a) {
+    extern __shared__ double sfl[];
     const int p = a.tile_prob[blockIdx.x];
     if (!a.stepping[p]) return;
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const int ncol = L.ny * L.nz, x0 = a.tile_off[blockIdx.x];
+    const int bx = min(brick_width(L), L.nx - x0);
+    const int gl = max(0, x0 - 2), gh = min(L.nx, x0 + bx + 2), nfx = gh - gl + 1;
+    const int ncell = bx * ncol;
+    // [q][col][face] x-faces, then [q][cell] y- and z-faces (cell = i + bx (j + ny k))
+    double *sX = sfl, *sY = sX + 5 * nfx * ncol, *sZ = sY + 5 * ncell;
+    const int src = wave_src(a);
+    const double *Uc = warr(a, I, UOFF + 5 * src);
+    BatchArgs b;
+    b.sp = a.sp;
+    b.gamma = a.gamma;
+    double F[5];
+    for (int t = threadIdx.x; t < nfx * ncol; t += blockDim.x) {
+        const int g = gl + t % nfx, col = t / nfx;
+        face_flux<0, INTERP, RS>(b, I, Uc, g, col % L.ny + NG, col / L.ny + NG, F);
+        for (int q = 0; q < 5; ++q) sX[(q * ncol + col) * nfx + (g - gl)] = F[q];
+    }
+    for (int t = threadIdx.x; t < ncell; t += blockDim.x) {
+        const int i = x0 + t % bx, col = t / bx, j = col % L.ny, k = col / L.ny;
+        face_flux<1, INTERP, RS>(b, I, Uc, j, i + NG, k + NG, F);
+        for (int q = 0; q < 5; ++q) sY[q * ncell + t] = F[q];
+        face_flux<2, INTERP, RS>(b, I, Uc, k, i + NG, j + NG, F);
+        for (int q = 0; q < 5; ++q) sZ[q * ncell + t] = F[q];
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t >= ncell) return;
+    const int il = t % bx, col = t / bx, j = col % L.ny, k = col / L.ny, i = x0 + il;
+    double r[5];
+    for (int q = 0; q < 5; ++q) {
+        const double *X = sX + (q * ncol + col) * nfx, *Y = sY + q * ncell, *Z = sZ + q * ncell;
+        auto fx = [&](int g) -> double {
+            g = wave_xface(I, g);
+            return g < 0 ? 0.0 : X[g - gl];
+        };
+        auto fy = [&](int jj) {
+            jj = jj < 0 ? jj + L.ny : (jj >= L.ny ? jj - L.ny : jj);
+            return Y[il + bx * (jj + L.ny * k)];
+        };
+        auto fz = [&](int kk) {
+            kk = kk < 0 ? kk + L.nz : (kk >= L.nz ? kk - L.nz : kk);
+            return Z[il + bx * (j + L.ny * kk)];
+        };
+        r[q] = wave_rhs(I, i, j, k, fx, fy, fz);
+    }
+    wave_finish(a, I, L.at(i + NG, j + NG, k + NG), wave_dst(a), src, r, a.dt[p]);
+}
+
+// shared memory of wave_brick_kernel for a problem (the largest brick)
+inline size_t brick_smem(const Layout &L) {
+    const int bx = std::min(brick_width(L), L.nx), ncol = L.ny * L.nz;
+    return sizeof(double) * 5 * ((size_t)std::min(bx + 5, L.nx + 1) * ncol + 2 * (size_t)bx * ncol);
+}
+
+// Within a run only two kinds of ghost cell are read: the x ghosts of
+// interior lines (by the x-face stencils) and the ghosts no fill reaches (by
+// their own zero-RHS update).  The others -- copies of interior cells,
+// constants -- are a function of the current state alone, so one fill at the
+// end of the run (wave_final_fill_kernel) gives them the values the per-stage
+// fill would have left.  This kernel lists the first two kinds once per run
+// (count only while list is null), in any order: each entry is filled
+// independently of the others.
+__global__ void __launch_bounds__(256) wave_ghost_list_kernel(WaveArgs a, int2 *list) {
+    const int p = a.tile_prob[blockIdx.x];
     const Inst &I = a.inst[p];
     const Layout &L = I.L;
     const long e = (long)a.tile_off[blockIdx.x] + threadIdx.x;
     if (e >= (long)L.sx * L.sy * L.sz) return;
     int cc[3] = {(int)(e % L.sx), (int)((e / L.sx) % L.sy), (int)(e / ((long)L.sx * L.sy))};
     if (is_interior(L, cc)) return;
-    const int ci = cc[0], cj = cc[1], ck = cc[2];
-    // Within a run only two kinds of ghost cell are read: the x ghosts of
-    // interior lines (by the x-face stencils) and the ghosts no fill reaches
-    // (by their own zero-RHS update).  The others -- copies of interior
-    // cells, constants -- are a function of the current state alone, so one
-    // fill at the end of the run (wave_final_fill_kernel) gives them the
-    // values the per-stage fill would have left.
-    const bool x_ghost_line = (ci < NG || ci >= L.nx + NG) && cj >= NG && cj < L.ny + NG && ck >= NG &&
-                              ck < L.nz + NG;
-    const int stage = a.stage, s0 = a.s0;
-    const int src = stage == 1 ? s0 : (stage == 2 ? (s0 + 1) % 3 : (s0 + 2) % 3);
-    const int dst = stage == 2 ? (s0 + 2) % 3 : (s0 + 1) % 3;
+    const bool x_ghost_line = (cc[0] < NG || cc[0] >= L.nx + NG) && cc[1] >= NG && cc[1] < L.ny + NG &&
+                              cc[2] >= NG && cc[2] < L.nz + NG;
+    BcInfo b;
+    for (int d = 0; d < 3; ++d) b.periodic[d] = I.periodic[d];
+    for (int f = 0; f < 6; ++f) b.bc[f] = I.bc[f];
+    int flip;
+    const int c0[3] = {cc[0], cc[1], cc[2]};
+    const int kind = resolve_source(L, b, cc, flip);
+    const bool unreached = kind == SRC_CELL && !is_interior(L, cc);
+    if (!x_ghost_line && !unreached) return;
+    // x ghosts of interior lines always resolve to an interior cell or a constant
+    const int cls = !unreached ? 0 : (cc[0] == c0[0] && cc[1] == c0[1] && cc[2] == c0[2] ? 1 : 2);
+    const int slot = atomicAdd(a.ghost_count + cls, 1);
+    if (list && slot < a.n_ghost[cls]) list[a.ghost_base[cls] + slot] = make_int2(p, (int)e);
+}
+
+// ghost fill of the stage's new state over the listed cells: the persistent
+// kernel's ghost phase for the cells a stage reads
+__global__ void __launch_bounds__(256) wave_ghost_kernel(WaveArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n_ghost[0]) return;
+    const int2 pe = a.ghosts[t];
+    const int p = pe.x;
+    if (!a.stepping[p]) return;
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const long e = pe.y;
+    int cc[3] = {(int)(e % L.sx), (int)((e / L.sx) % L.sy), (int)(e / ((long)L.sx * L.sy))};
+    const long o = L.at(cc[0], cc[1], cc[2]);
+    const int dst = wave_dst(a);
     BcInfo b;
     for (int d = 0; d < 3; ++d) b.periodic[d] = I.periodic[d];
     for (int f = 0; f < 6; ++f) b.bc[f] = I.bc[f];
     int flip;
     const int kind = resolve_source(L, b, cc, flip);
-    const bool unreached = kind == SRC_CELL && !is_interior(L, cc);
-    if (!x_ghost_line && !unreached) return;
     double Wn[5];
     if (kind != SRC_CELL) {
         special_state(kind, Wn);
-    } else if (!unreached) {
+    } else {
         const long s = L.at(cc[0], cc[1], cc[2]);
         for (int q = 0; q < 5; ++q) Wn[q] = warr(a, I, 5 * dst + q)[s];
-    } else {
-        // a ghost cell no fill reaches keeps its own stage update with rhs = 0
-        const long s = L.at(cc[0], cc[1], cc[2]);
-        double Un[5];
-        for (int q = 0; q < 5; ++q)
-            Un[q] = rk_combine(stage, warr(a, I, UOFF + 5 * s0 + q)[s], warr(a, I, UOFF + 5 * src + q)[s], 0.0, a.dt[p]);
-        c2p_exact(Un, a.gamma, Wn);
     }
     apply_flips(flip, Wn);
-    const long o = L.at(ci, cj, ck);
     double Ud[5];
     p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
     for (int q = 0; q < 5; ++q) { warr(a, I, 5 * dst + q)[o] = Wn[q]; warr(a, I, UOFF + 5 * dst + q)[o] = Ud[q]; }
+}
+
+// The window's steps of the ghost cells no fill reaches that are their own
+// source: per step the three stage updates with rhs = 0 and runge_kutta_3's
+// c2p -> p2c round trip, as every stage of the persistent kernel applies them,
+// from the step-start buffer of the window (s_begin) into the buffer holding
+// the problem's state at the window's end.
+__global__ void __launch_bounds__(256) wave_unreached_kernel(WaveArgs a, int nsteps, int s_begin) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n_ghost[1]) return;
+    const int2 pe = a.ghosts[a.ghost_base[1] + t];
+    const int p = pe.x;
+    if (nsteps < 1 || a.dt_hist[p] < 0.0) return;  // the problem did not step in this window
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const long e = pe.y;
+    const long o = L.at((int)(e % L.sx), (int)((e / L.sx) % L.sy), (int)(e / ((long)L.sx * L.sy)));
+    double U0[5], U[5], Wn[5];
+    for (int q = 0; q < 5; ++q) U0[q] = warr(a, I, UOFF + 5 * s_begin + q)[o];
+    for (int w = 0; w < nsteps; ++w) {
+        const double dt = a.dt_hist[(long)w * a.n_prob + p];
+        if (dt < 0.0) break;
+        for (int q = 0; q < 5; ++q) U[q] = U0[q];
+        for (int stage = 1; stage <= 3; ++stage) {
+            double Un[5];
+            for (int q = 0; q < 5; ++q) Un[q] = rk_combine(stage, U0[q], U[q], 0.0, dt);
+            c2p_exact(Un, a.gamma, Wn);
+            p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, U);
+        }
+        for (int q = 0; q < 5; ++q) U0[q] = U[q];
+    }
+    const int buf = a.state_out[p];
+    for (int q = 0; q < 5; ++q) { warr(a, I, 5 * buf + q)[o] = Wn[q]; warr(a, I, UOFF + 5 * buf + q)[o] = U0[q]; }
+}
+
+// The ghost cells no fill reaches whose source is another such cell: its last
+// stage's state with the sign flips, after wave_unreached_kernel
+__global__ void __launch_bounds__(256) wave_unreached_copy_kernel(WaveArgs a, int nsteps) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.n_ghost[2]) return;
+    const int2 pe = a.ghosts[a.ghost_base[2] + t];
+    const int p = pe.x;
+    if (nsteps < 1 || a.dt_hist[p] < 0.0) return;
+    const Inst &I = a.inst[p];
+    const Layout &L = I.L;
+    const long e = pe.y;
+    int cc[3] = {(int)(e % L.sx), (int)((e / L.sx) % L.sy), (int)(e / ((long)L.sx * L.sy))};
+    const long o = L.at(cc[0], cc[1], cc[2]);
+    BcInfo b;
+    for (int d = 0; d < 3; ++d) b.periodic[d] = I.periodic[d];
+    for (int f = 0; f < 6; ++f) b.bc[f] = I.bc[f];
+    int flip;
+    resolve_source(L, b, cc, flip);
+    const long s = L.at(cc[0], cc[1], cc[2]);
+    const int buf = a.state_out[p];
+    double Wn[5], Ud[5];
+    for (int q = 0; q < 5; ++q) Wn[q] = warr(a, I, 5 * buf + q)[s];
+    apply_flips(flip, Wn);
+    p2c_exact(Wn[0], Wn[1], Wn[2], Wn[3], Wn[4], a.gamma, Ud);
+    for (int q = 0; q < 5; ++q) { warr(a, I, 5 * buf + q)[o] = Wn[q]; warr(a, I, UOFF + 5 * buf + q)[o] = Ud[q]; }
 }
 
 // The ghost cells the per-stage fill leaves out, once at the end of a run:
@@ -593,8 +785,13 @@ struct ns3d_batch {
     void *wave = nullptr;
     unsigned long long *w_minbits = nullptr;
     double *w_dt = nullptr;
-    int *w_stepping = nullptr, *w_tiles = nullptr;  // tiles: [interior prob | interior off | box prob | box off]
+    int *w_stepping = nullptr, *w_tiles = nullptr;  // tiles: [interior prob | off | box prob | off | brick prob | x0]
     long w_tile_cap = 0;
+    int2 *w_ghosts = nullptr;    // WaveArgs::ghosts (wave_ghost_list_kernel), built once
+    int w_n_ghost[3] = {-1, 0, 0};
+    int *w_ghost_count = nullptr;
+    double *w_dt_hist = nullptr;
+    size_t w_brick_smem = 0;     // wave_brick_kernel's dynamic shared memory (largest brick)
     cudaGraphExec_t graph = nullptr;
     int graph_max_steps = -1;
     SchemeParams<double> sp;
@@ -672,28 +869,49 @@ WaveArgs wave_args(ns3d_batch *b, int max_steps) {
     a.state_out = b->d_state; a.stepping = b->w_stepping; a.max_steps = max_steps;
     a.s0 = 0; a.stage = 0;
     a.tile_prob = nullptr; a.tile_off = nullptr;
+    a.ghosts = b->w_ghosts;
+    a.ghost_count = b->w_ghost_count;
+    for (int k = 0, base = 0; k < 3; ++k) {
+        a.n_ghost[k] = std::max(0, b->w_n_ghost[k]);
+        a.ghost_base[k] = base;
+        base += a.n_ghost[k];
+    }
+    a.dt_hist = b->w_dt_hist;
+    a.hist_slot = 0;
+    a.n_prob = b->n;
     return a;
 }
 
 // Tile tables of the listed problems: 256 cells per block, interior cells
-// (faces, update, CFL) and whole boxes (ghost fill, initial conversion).
-int wave_tables(ns3d_batch *b, const std::vector<int> &probs, int &n_int, int &n_box) {
-    std::vector<int> ip, io, bp, bo;
+// (CFL, and faces + update of problems too wide for bricks), whole boxes
+// (initial conversion, ghost list, final fill), and bricks of brick_width
+// x-cells by the cross-section (wave_brick_kernel).
+struct WaveTiles {
+    int n_int = 0, n_box = 0, n_brick = 0;
+    bool general = false;  // a listed problem takes the separate face and update kernels
+};
+
+int wave_tables(ns3d_batch *b, const std::vector<int> &probs, WaveTiles &wt) {
+    std::vector<int> ip, io, bp, bo, kp, ko;
+    wt.general = false;
     for (int p : probs) {
         const Layout &L = b->inst[p].L;
         const long ni = (long)L.nx * L.ny * L.nz, nb = (long)L.sx * L.sy * L.sz;
         for (long o = 0; o < ni; o += 256) { ip.push_back(p); io.push_back((int)o); }
         for (long o = 0; o < nb; o += 256) { bp.push_back(p); bo.push_back((int)o); }
+        if (brick_ok(L)) {
+            for (int x0 = 0; x0 < L.nx; x0 += brick_width(L)) { kp.push_back(p); ko.push_back(x0); }
+        } else {
+            wt.general = true;
+        }
     }
-    n_int = (int)ip.size();
-    n_box = (int)bp.size();
-    if ((long)(n_int + n_box) * 2 > b->w_tile_cap) return bfail(b, NS3D_ERR_STATE, "tile table capacity");
+    wt.n_int = (int)ip.size();
+    wt.n_box = (int)bp.size();
+    wt.n_brick = (int)kp.size();
+    if ((long)(wt.n_int + wt.n_box + wt.n_brick) * 2 > b->w_tile_cap) return bfail(b, NS3D_ERR_STATE, "tile table capacity");
     std::vector<int> all;
-    all.reserve(2 * (n_int + n_box));
-    all.insert(all.end(), ip.begin(), ip.end());
-    all.insert(all.end(), io.begin(), io.end());
-    all.insert(all.end(), bp.begin(), bp.end());
-    all.insert(all.end(), bo.begin(), bo.end());
+    all.reserve(2 * (wt.n_int + wt.n_box + wt.n_brick));
+    for (const std::vector<int> *v : {&ip, &io, &bp, &bo, &kp, &ko}) all.insert(all.end(), v->begin(), v->end());
     if (!all.empty())
         BCK(b, cudaMemcpyAsync(b->w_tiles, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream),
             "tile tables");
@@ -704,19 +922,57 @@ int wave_tables(ns3d_batch *b, const std::vector<int> &probs, int &n_int, int &n
 int ensure_wave(ns3d_batch *b) {
     if (b->wave) return NS3D_OK;
     long tiles = 0;
+    size_t smem = 0;
     for (const Inst &I : b->inst) {
         const Layout &L = I.L;
         tiles += ((long)L.nx * L.ny * L.nz + 255) / 256 + ((long)L.sx * L.sy * L.sz + 255) / 256;
+        if (brick_ok(L)) {
+            tiles += (L.nx + brick_width(L) - 1) / brick_width(L);
+            smem = std::max(smem, brick_smem(L));
+        }
     }
     b->w_tile_cap = 2 * tiles;
     const size_t n = (size_t)b->n;
-    const size_t bytes = n * 8 + n * 8 + n * 4 + (size_t)b->w_tile_cap * 4 + 4 * 256;
+    const size_t bytes = n * 8 + n * 8 + n * 4 + 256 + n * 8 * WAVE_WINDOW + 256 + (size_t)b->w_tile_cap * 4 + 4 * 256;
     BCK(b, cudaMalloc(&b->wave, bytes), "wavefront tables");
     char *p = (char *)b->wave;
     b->w_minbits = (unsigned long long *)p; p += (n * 8 + 255) / 256 * 256;
     b->w_dt = (double *)p; p += (n * 8 + 255) / 256 * 256;
     b->w_stepping = (int *)p; p += (n * 4 + 255) / 256 * 256;
+    b->w_ghost_count = (int *)p; p += 256;
+    b->w_dt_hist = (double *)p; p += (n * 8 * WAVE_WINDOW + 255) / 256 * 256;
     b->w_tiles = (int *)p;
+    b->w_brick_smem = smem;
+    if (smem > 48 * 1024) {
+        BCK(b, cudaFuncSetAttribute(wave_brick_kernel<I_WENO5, R_ROE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+            "brick shared memory");
+        BCK(b, cudaFuncSetAttribute(wave_brick_kernel<RUNTIME, RUNTIME>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem),
+            "brick shared memory");
+    }
+    return NS3D_OK;
+}
+
+// the ghost-cell lists (once per batch: they depend on the layouts and
+// boundary types only); the box tiles of every problem are set
+int build_ghost_list(ns3d_batch *b, WaveArgs &a, int n_box) {
+    if (b->w_n_ghost[0] >= 0) return NS3D_OK;
+    int count[3] = {0, 0, 0};
+    for (int pass = 0; pass < 2; ++pass) {
+        BCK(b, cudaMemsetAsync(b->w_ghost_count, 0, 3 * sizeof(int), b->stream), "ghost count");
+        a.ghost_count = b->w_ghost_count;
+        for (int k = 0, base = 0; k < 3; ++k) { a.n_ghost[k] = count[k]; a.ghost_base[k] = base; base += count[k]; }
+        wave_ghost_list_kernel<<<n_box, 256, 0, b->stream>>>(a, pass ? b->w_ghosts : nullptr);
+        BCK(b, cudaGetLastError(), "ghost list");
+        BCK(b, cudaMemcpyAsync(count, b->w_ghost_count, 3 * sizeof(int), cudaMemcpyDeviceToHost, b->stream),
+            "ghost count");
+        BCK(b, cudaStreamSynchronize(b->stream), "synchronize");
+        const size_t total = (size_t)count[0] + count[1] + count[2];
+        if (pass == 0 && total == 0) break;
+        if (pass == 0) BCK(b, cudaMalloc(&b->w_ghosts, sizeof(int2) * total), "ghost list");
+    }
+    for (int k = 0; k < 3; ++k) b->w_n_ghost[k] = count[k];
+    a = wave_args(b, a.max_steps);
     return NS3D_OK;
 }
 
@@ -729,21 +985,38 @@ int run_wave(ns3d_batch *b, int max_steps) {
     WaveArgs a = wave_args(b, max_steps);
     std::vector<int> active(b->n);
     for (int p = 0; p < b->n; ++p) active[p] = p;
-    int n_int = 0, n_box = 0;
-    if ((r = wave_tables(b, active, n_int, n_box))) return r;
-    auto set_tables = [&](bool box) {
-        a.tile_prob = b->w_tiles + (box ? 2 * n_int : 0);
-        a.tile_off = b->w_tiles + (box ? 2 * n_int + n_box : n_int);
+    WaveTiles wt;
+    if ((r = wave_tables(b, active, wt))) return r;
+    // table views: 0 interior, 1 box, 2 brick
+    auto set_tables = [&](int which) {
+        const int off[3] = {0, 2 * wt.n_int, 2 * (wt.n_int + wt.n_box)};
+        const int len[3] = {wt.n_int, wt.n_box, wt.n_brick};
+        a.tile_prob = b->w_tiles + off[which];
+        a.tile_off = b->w_tiles + off[which] + len[which];
     };
-    set_tables(true);
-    wave_init_kernel<<<n_box, 256, 0, b->stream>>>(a);
+    set_tables(1);
+    wave_init_kernel<<<wt.n_box, 256, 0, b->stream>>>(a);
     BCK(b, cudaGetLastError(), "wavefront init");
+    if ((r = build_ghost_list(b, a, wt.n_box))) return r;
+    set_tables(1);
     const unsigned pblocks = (unsigned)((b->n + 127) / 128);
+    const unsigned gblocks = (unsigned)((a.n_ghost[0] + 255) / 256);
+    // the unreached ghost cells' steps since the last catch-up, from the
+    // step-start buffer at that point
+    int s_begin = 0, wsteps = 0;
+    auto catch_up = [&]() {
+        if (wsteps == 0) return;
+        if (a.n_ghost[1]) wave_unreached_kernel<<<(a.n_ghost[1] + 255) / 256, 256, 0, b->stream>>>(a, wsteps, s_begin);
+        if (a.n_ghost[2]) wave_unreached_copy_kernel<<<(a.n_ghost[2] + 255) / 256, 256, 0, b->stream>>>(a, wsteps);
+        wsteps = 0;
+    };
     const bool weno_roe = b->sp.interp == I_WENO5 && b->sp.riemann == R_ROE;
     std::vector<int> status(b->n), steps(b->n);
     int s0 = 0;
     for (int step = 0; step < max_steps; ++step) {
-        if (step > 0 && step % 16 == 0) {
+        if (step > 0 && step % WAVE_WINDOW == 0) {
+            catch_up();
+            s_begin = s0;
             BCK(b, cudaMemcpyAsync(status.data(), b->d_status, sizeof(int) * b->n, cudaMemcpyDeviceToHost, b->stream),
                 "statuses");
             BCK(b, cudaMemcpyAsync(steps.data(), b->d_steps, sizeof(int) * b->n, cudaMemcpyDeviceToHost, b->stream),
@@ -755,32 +1028,41 @@ int run_wave(ns3d_batch *b, int max_steps) {
             if (act.empty()) break;
             if (act.size() != active.size()) {
                 active.swap(act);
-                if ((r = wave_tables(b, active, n_int, n_box))) return r;
+                if ((r = wave_tables(b, active, wt))) return r;
             }
         }
         a.s0 = s0;
-        set_tables(false);
-        wave_cfl_kernel<<<n_int, 256, 0, b->stream>>>(a);
+        a.hist_slot = wsteps;
+        set_tables(0);
+        wave_cfl_kernel<<<wt.n_int, 256, 0, b->stream>>>(a);
         wave_schedule_kernel<<<pblocks, 128, 0, b->stream>>>(a, b->n);
         for (int stage = 1; stage <= 3; ++stage) {
             a.stage = stage;
-            set_tables(false);
-            if (weno_roe) wave_face_kernel<I_WENO5, R_ROE><<<n_int, 256, 0, b->stream>>>(a);
-            else wave_face_kernel<RUNTIME, RUNTIME><<<n_int, 256, 0, b->stream>>>(a);
-            wave_update_kernel<<<n_int, 256, 0, b->stream>>>(a);
-            set_tables(true);
-            wave_ghost_kernel<<<n_box, 256, 0, b->stream>>>(a);
+            if (wt.n_brick) {
+                set_tables(2);
+                if (weno_roe) wave_brick_kernel<I_WENO5, R_ROE><<<wt.n_brick, 256, b->w_brick_smem, b->stream>>>(a);
+                else wave_brick_kernel<RUNTIME, RUNTIME><<<wt.n_brick, 256, b->w_brick_smem, b->stream>>>(a);
+            }
+            if (wt.general) {
+                set_tables(0);
+                if (weno_roe) wave_face_kernel<I_WENO5, R_ROE><<<wt.n_int, 256, 0, b->stream>>>(a);
+                else wave_face_kernel<RUNTIME, RUNTIME><<<wt.n_int, 256, 0, b->stream>>>(a);
+                wave_update_kernel<<<wt.n_int, 256, 0, b->stream>>>(a);
+            }
+            if (gblocks) wave_ghost_kernel<<<gblocks, 256, 0, b->stream>>>(a);
         }
         s0 = (s0 + 1) % 3;
         wave_post_kernel<<<pblocks, 128, 0, b->stream>>>(a, b->n, s0);
         BCK(b, cudaGetLastError(), "wavefront step");
+        ++wsteps;
     }
+    catch_up();
     // the ghost cells left out of the per-stage fills, every problem
     std::vector<int> all(b->n);
     for (int p = 0; p < b->n; ++p) all[p] = p;
-    if ((r = wave_tables(b, all, n_int, n_box))) return r;
-    set_tables(true);
-    wave_final_fill_kernel<<<n_box, 256, 0, b->stream>>>(a);
+    if ((r = wave_tables(b, all, wt))) return r;
+    set_tables(1);
+    wave_final_fill_kernel<<<wt.n_box, 256, 0, b->stream>>>(a);
     BCK(b, cudaGetLastError(), "final ghost fill");
     BCK(b, cudaStreamSynchronize(b->stream), "synchronize");
     return NS3D_OK;
@@ -891,6 +1173,7 @@ int ns3d_batch_destroy(ns3d_batch *b) {
     if (b->pool) cudaFree(b->pool);
     if (b->meta) cudaFree(b->meta);
     if (b->wave) cudaFree(b->wave);
+    if (b->w_ghosts) cudaFree(b->w_ghosts);
     delete b;
     return NS3D_OK;
 }
@@ -943,7 +1226,7 @@ int ns3d_batch_run(ns3d_batch *b, int max_steps) {
     return NS3D_OK;
 }
 
-int ns3d_batch_autotune(ns3d_batch *b, int trial_steps, int out[2]) {
+int ns3d_batch_autotune(ns3d_batch *b, int trial_steps, int out[3]) {
     if (!b || trial_steps < 1) return NS3D_ERR_INVALID_ARG;
     cudaSetDevice(b->device);
     // save the state (a device copy), try each configuration for trial_steps

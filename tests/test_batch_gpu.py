@@ -100,3 +100,42 @@ def test_autotune_picks_a_valid_config_and_keeps_the_state(gpu_lib):
         b.run()
         W, t, steps = oracle_run(P, grids[0], states[0], t_end[0])
         assert max(rel_linf(a, r) for a, r in zip(b.primitives(0), W)) <= 1e-10
+
+
+def test_wavefront_bricks_and_wide_cross_sections(gpu_lib):
+    """Cross-sections of up to 64 cells take the fused brick kernel, wider ones
+    the separate face and update kernels; both in one batch, with walls in x
+    (sign flips in the ghost fill) and a state that varies in y and z.  Every
+    problem equals the persistent schedule bit for bit and the oracle."""
+    P, _ = make_params(n=(8, 4, 4), Ma=1.0, Re=math.inf, cfl=0.5, dt_fixed=-1.0, interpolation=0, riemann=0,
+                       bcs=(1, 3, 0, 0, 0, 0))
+    shapes = [(30, 4, 4), (26, 8, 8), (22, 9, 9), (18, 3, 5), (40, 3, 3)]
+    rng = np.random.default_rng(7)
+    grids, states, t_end = [], [], []
+    for nx, ny, nz in shapes:
+        grids.append(GridDesc(global_nx=nx, global_ny=ny, global_nz=nz, Lx=1.0, Ly=1.0, Lz=1.0))
+        left = (rng.uniform(0.5, 1.0), rng.uniform(-0.5, 0.5), rng.uniform(0.5, 2.0))
+        right = (rng.uniform(0.1, 0.5), rng.uniform(-0.5, 0.5), rng.uniform(0.1, 0.5))
+        rho, u, v, w, p = shock_tube_state(nx, ny, nz, left, right)
+        shp = rho.shape
+        rho = rho * (1 + 0.05 * rng.standard_normal(shp))
+        v = 0.1 * rng.standard_normal(shp)
+        w = 0.1 * rng.standard_normal(shp)
+        states.append((rho, u, v, w, p))
+        t_end.append(rng.uniform(0.02, 0.03))
+    outs = []
+    for cfg in [(0, 256, 1), (2, 256, 2)]:
+        with Batch(P, grids, t_end) as b:
+            for i, st in enumerate(states):
+                b.set_interior_primitives(i, *st)
+            b.set_config(*cfg)
+            b.run()
+            outs.append([b.primitives(i) for i in range(len(grids))])
+            queries = [b.query(i) for i in range(len(grids))]
+    for a, r in zip(outs[0], outs[1]):
+        assert np.array_equal(a, r)
+    for i in (1, 2):  # a brick problem and a wide one against the oracle
+        W, t, steps = oracle_run(P, grids[i], states[i], t_end[i])
+        tg, sg, status = queries[i]
+        assert status == 0 and sg == steps and abs(tg - t) <= 1e-14
+        assert max(rel_linf(a, r) for a, r in zip(outs[0][i], W)) <= 1e-10
