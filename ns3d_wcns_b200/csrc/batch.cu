@@ -501,9 +501,11 @@ __global__ void __launch_bounds__(256) wave_update_kernel(WaveArgs a) {
 // z-faces go to shared memory, then each thread updates one cell from them.
 // The same face_flux and update arithmetic as wave_face_kernel +
 // wave_update_kernel, so the same bits, without the global face arrays'
-// round trip and one launch per stage fewer.
+// round trip and one launch per stage fewer.  Registers are capped for three
+// resident blocks per SM (80 registers, a few spills): measured faster than
+// two blocks at 98 registers on the 512-tube benchmark.
 template <int INTERP, int RS>
-__global__ void __launch_bounds__(256) wave_brick_kernel(WaveArgs a) {
+__global__ void __launch_bounds__(256, 3) wave_brick_kernel(WaveArgs a) {
     extern __shared__ double sfl[];
     const int p = a.tile_prob[blockIdx.x];
     if (!a.stepping[p]) return;
