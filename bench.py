@@ -356,8 +356,14 @@ def batched_report(device: int, n: int = 512, check=((200, 8, "reference"), (400
             sel = [i for i, g in enumerate(grids) if g.global_nx == nx][:count]
             idx += sel
             jobs += [(nx, tuple(left[i]), tuple(right[i]), float(t_end[i]), which) for i in sel]
+        # longest tubes first, one job at a time, so that the pool's wall time
+        # is close to the longest single run
+        order = sorted(range(len(jobs)), key=lambda j: -jobs[j][0])
         with mp.get_context("spawn").Pool(min(len(jobs), cores)) as pool:
-            refs = pool.map(_ref_tube, jobs)
+            done = pool.map(_ref_tube, [jobs[j] for j in order], chunksize=1)
+        refs = [None] * len(jobs)
+        for j, r in zip(order, done):
+            refs[j] = r
         per_nx, rate = {}, []
         for i, (Wr, sec, st, kind) in zip(idx, refs):
             Wg = b.primitives(i)
@@ -636,6 +642,13 @@ def main():
     ap.add_argument("--batch-problems", type=int, default=512)
     ap.add_argument("--batched-check", action="store_true",
                     help="batched report only, checking every Nx=200 problem and 8 of each larger Nx")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="run this many host-loop RK3 steps of the workload at --n (plain FP64, or the mixed "
+                         "path with --no-fp64) and exit: the case for one-kernel profiler captures")
+    ap.add_argument("--no-fp64", action="store_true", help="with --profile-steps: the mixed path")
+    ap.add_argument("--batch-profile", type=int, default=0,
+                    help="run the first --batch-problems shock tubes of the batched benchmark for this many "
+                         "steps (wavefront schedule, no checks) and exit: the case for profiler captures")
     ap.add_argument("--accuracy", default="", help="comma-separated grid sizes: accuracy report only")
     ap.add_argument("--accuracy-ref", type=int, default=0, help="also the reference CPU time series at this size")
     args = ap.parse_args()
@@ -655,6 +668,38 @@ def main():
                              check=((200, 10 ** 6, "port"), (400, 8, "port"), (800, 8, "port"), (1600, 8, "port"),
                                     (200, 8, "reference")))
         print(json.dumps({"batched": rep}))
+        return
+    if args.batch_profile:
+        import math
+        import torch
+        from ns3d_wcns_b200.batch import Batch, shock_tube_problems
+        from ns3d_wcns_b200.config import make_params
+        from ns3d_wcns_b200.initial import shock_tube_state
+        torch.cuda.set_device(local)
+        P, _ = make_params(n=(8, 4, 4), Ma=1.0, Re=math.inf, cfl=0.5, dt_fixed=-1.0, interpolation=0, riemann=0,
+                           bcs=(3, 3, 0, 0, 0, 0))
+        grids, left, right, t_end = shock_tube_problems(args.batch_problems, seed=5)
+        with Batch(P, grids, t_end, device=local) as b:
+            for i, g in enumerate(grids):
+                b.set_interior_primitives(i, *shock_tube_state(g.global_nx, 4, 4, left[i], right[i]))
+            b.set_config(0, 256, 1)
+            b.run(args.batch_profile)
+        print(json.dumps({"batch_profile": args.batch_profile, "problems": args.batch_problems}))
+        return
+    if args.profile_steps:
+        import torch
+        from ns3d_wcns_b200.initial import isotropic_state
+        from ns3d_wcns_b200.solver import Solver
+        torch.cuda.set_device(local)
+        P, G = bench_params(args.n, 1 if args.no_fp64 else 0)
+        with Solver(P, G, device=local) as s:
+            stream = torch.cuda.Stream()
+            s.set_stream(stream.cuda_stream)
+            s.set_interior_primitives(*isotropic_state((args.n,) * 3, 1.4, 0.3, seed=0))
+            for _ in range(args.profile_steps):
+                s.rk3_step(s.compute_timestep())
+            s.synchronize()
+        print(json.dumps({"profile_steps": args.profile_steps, "n": args.n, "mixed": bool(args.no_fp64)}))
         return
     if args.accuracy:
         rep = accuracy_report(local, sizes=[int(x) for x in args.accuracy.split(",")], ref_n=args.accuracy_ref)
@@ -774,6 +819,23 @@ def main():
             if len(f) == 2 and not ln.startswith("#") and f[0] == dom:
                 traffic = float(f[1])
 
+    # FP64 pipe of the dominant kernel: its FP64 thread instructions per cell
+    # (one-launch ncu capture, profiles/fp64_instr_per_cell_192.txt) over the
+    # event time, against 64 FP64 lanes per SM per clock at the sampled clock
+    fp64_pipe = None
+    fpath = os.path.join(ROOT, "profiles", "fp64_instr_per_cell_192.txt")
+    if os.path.exists(fpath):
+        for ln in open(fpath):
+            f = ln.split("#")[0].split()
+            if len(f) == 2 and f[0] == dom:
+                sms = torch.cuda.get_device_properties(local).multi_processor_count
+                mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+                rate = float(f[1]) * cells / (avg_ms * 1e-3)
+                peak64 = sms * 64 * mhz * 1e6
+                fp64_pipe = {"achieved": rate, "peak": peak64, "unit": "FP64 thread-instructions/s",
+                             "frac": rate / peak64, "fp64_instr_per_cell": float(f[1]),
+                             "source": "profiles/fp64_instr_per_cell_192.txt (ncu, one launch at 192^3)"}
+
     # end to end through the C ABI with host buffers (pinned)
     e2e = e2e_full = None
     if not args.no_e2e:
@@ -882,7 +944,7 @@ def main():
             "e2e": e2e, "e2e_full_state": e2e_full, "mixed": mixed, "grid_512": g512,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                         "algorithmic_bytes_per_cell": algo_bytes_per_cell.get(dom)},
+                         "algorithmic_bytes_per_cell": algo_bytes_per_cell.get(dom), "fp64_pipe": fp64_pipe},
             "kernels_ms": {k: round(v["ms"] / max(v["launches"], 1), 4) for k, v in prof.items()},
             "kernels_ms_source": "CUDA events around each kernel, on the launching stream, in a pass of the same "
                                  "number of steps right after the timed region (the timed region runs the graph-"

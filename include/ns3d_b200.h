@@ -217,8 +217,11 @@ int ns3d_profile_report(ns3d_handle *h, char *buf, long len);
 /* ------------------------------------------------------------- adjoint
  * Hand-written reverse mode of the RHS and of the RK3 step (no counterpart in
  * the reference).  Plain FP64 path, periodic boundaries, component-wise
- * WENO5 / MDCD_LINEAR interpolation with the Roe, Rusanov or HLL flux; other
- * configurations return NS3D_ERR_CONFIG.  The state differentiated is the
+ * WENO5 / MDCD_LINEAR / MDCD_HYBRID interpolation (interpolation.cpp:86-209;
+ * the hybrid's detector is a switch with zero derivative, its active branch
+ * is differentiated) with the Roe, Rusanov, HLL or HLLC flux
+ * (InviscousFlux.cpp:449-592: the active arms of the wave-speed and star-state
+ * branches); other configurations return NS3D_ERR_CONFIG.  The state differentiated is the
  * interior conserved field (the c2p/p2c round trip is the identity).
  * Host arrays are Field3D-sized (sx*sy*sz); only interior entries are read,
  * ghost entries of outputs are zero. */
@@ -250,7 +253,9 @@ int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int check
  * atomic work queue, largest first (the persistent schedule).  The
  * wavefront schedule (cluster 0) instead advances every active problem one
  * step per round of flat launches over all their cells, so uneven sizes
- * keep the whole GPU busy; the host drops finished problems every 16 steps.
+ * keep the whole GPU busy (faces and update fused per brick of 256/(ny nz)
+ * x-cells by the cross-section when ny nz <= 64); the host drops finished
+ * problems every 16 steps.
  * Both give the same bits.  ns3d_batch_autotune times the wavefront and the
  * persistent cluster size (1,2,4,8) x CTA width (128,256) x resident CTAs
  * per SM (1,2,3: the register budget of the kernel instantiation) choices
@@ -263,7 +268,9 @@ int ns3d_batch_destroy(ns3d_batch *b);
 const char *ns3d_batch_last_error(const ns3d_batch *b);
 /* interior primitives of problem i (nx*ny*nz each) + its ghost fill */
 int ns3d_batch_set_interior_primitives(ns3d_batch *b, int problem, const double *const fields[5]);
-/* one persistent launch (captured in a CUDA graph) to every problem's t_end */
+/* every problem to its t_end (or max_steps steps) with the configured
+ * schedule: the wavefront's rounds of launches, or one persistent launch
+ * captured in a CUDA graph */
 int ns3d_batch_run(ns3d_batch *b, int max_steps);
 int ns3d_batch_autotune(ns3d_batch *b, int trial_steps, int config_out[3]);
 int ns3d_batch_set_config(ns3d_batch *b, int cluster, int threads, int ctas_per_sm);
@@ -278,12 +285,14 @@ int ns3d_batch_download(ns3d_batch *b, int problem, double *const out[5]);
  * ns3d_debug_face_vjp: U30 = conserved stencil U[q][m] (q = rho..E, m = cells
  * i-2..i+3), Fbar5 = adjoint of the face flux; out30 = dF/dU^T Fbar (same
  * indexing); flux5 (nullable) = the production face flux of that stencil.
- * interpolation: NS3D_WENO5 | NS3D_MDCD_LINEAR (lin = its six coefficients);
- * riemann: NS3D_ROE | NS3D_RUSANOV | NS3D_HLL.
+ * interpolation: NS3D_WENO5 | NS3D_MDCD_LINEAR (lin = its six coefficients)
+ * | NS3D_MDCD_HYBRID (lin = ten values: the six linear coefficients, then the
+ * four of the WENO branch); riemann: NS3D_ROE | NS3D_RUSANOV | NS3D_HLLC |
+ * NS3D_HLL.
  * ns3d_debug_visc_vjp: pointwise node viscous flux at x4 = (u,v,w,T) with
  * gradients g12 (d{u,v,w,T}/d{x,y,z}); V9 (nullable) = the nine fluxes
  * txx tyy tzz txy txz tyz ex ey ez, xb4/gb12 = their VJP with Vbar9. */
-int ns3d_debug_face_vjp(int direction, int interpolation, int riemann, double gamma, const double lin[6],
+int ns3d_debug_face_vjp(int direction, int interpolation, int riemann, double gamma, const double *lin,
                         const double *U30, const double *Fbar5, double *out30, double *flux5);
 int ns3d_debug_visc_vjp(double mu0, double S, double cp_over_pr, const double *x4, const double *g12,
                         const double *Vbar9, double *xb4, double *gb12, double *V9);

@@ -478,7 +478,7 @@ void riemann_flux_host(const SchemeParams<double> &sp, const double *UL, const d
 }  // namespace ns3d
 
 extern "C" int ns3d_debug_face_vjp(int direction, int interpolation, int riemann, double gamma,
-                                   const double lin[6], const double *U30, const double *Fbar5, double *out30,
+                                   const double *lin, const double *U30, const double *Fbar5, double *out30,
                                    double *flux5) {
     using namespace ns3d;
     if (!U30 || !Fbar5 || !out30 || direction < 0 || direction > 2) return -1;
