@@ -334,8 +334,12 @@ constexpr int WAVE_WINDOW = 16;
 // face + update kernel (wave_brick_kernel) on bricks of 256 / (ny nz) x-cells
 // by the whole cross-section; larger cross-sections the separate kernels.
 constexpr int BRICK_COLS = 64;
+#ifndef NS3D_BRICK_CELLS
+#define NS3D_BRICK_CELLS 512
+#endif
+constexpr int BRICK_CELLS = NS3D_BRICK_CELLS;  // cells per brick (256 threads: two cells each)
 __host__ __device__ __forceinline__ bool brick_ok(const Layout &L) { return L.ny * L.nz <= BRICK_COLS; }
-__host__ __device__ __forceinline__ int brick_width(const Layout &L) { return 256 / (L.ny * L.nz); }
+__host__ __device__ __forceinline__ int brick_width(const Layout &L) { return BRICK_CELLS / (L.ny * L.nz); }
 
 __device__ __forceinline__ double *warr(const WaveArgs &a, const Inst &I, int q) {
     return a.pool + I.base + (long)q * I.L.plane;
@@ -495,10 +499,11 @@ __global__ void __launch_bounds__(256) wave_update_kernel(WaveArgs a) {
     wave_finish(a, I, L.at(i + NG, j + NG, k + NG), wave_dst(a), wave_src(a), r, a.dt[p]);
 }
 
-// Faces and update of one brick -- bx x-cells by the whole ny x nz
-// cross-section of one problem -- in one kernel: the brick's x-faces (with
-// the 2 + 3 faces beyond its ends the difference stencil needs), y-faces and
-// z-faces go to shared memory, then each thread updates one cell from them.
+// Faces and update of one brick -- bx = BRICK_CELLS / (ny nz) x-cells by the
+// whole ny x nz cross-section of one problem -- in one kernel: the brick's
+// x-faces (with the 2 + 3 faces beyond its ends the difference stencil
+// needs), y-faces and z-faces go to shared memory, then the threads update
+// the brick's cells from them.
 // The same face_flux and update arithmetic as wave_face_kernel +
 // wave_update_kernel, so the same bits, without the global face arrays'
 // round trip and one launch per stage fewer.  Registers are capped for three
@@ -536,27 +541,27 @@ __global__ void __launch_bounds__(256, 3) wave_brick_kernel(WaveArgs a) {
         for (int q = 0; q < 5; ++q) sZ[q * ncell + t] = F[q];
     }
     __syncthreads();
-    const int t = threadIdx.x;
-    if (t >= ncell) return;
-    const int il = t % bx, col = t / bx, j = col % L.ny, k = col / L.ny, i = x0 + il;
-    double r[5];
-    for (int q = 0; q < 5; ++q) {
-        const double *X = sX + (q * ncol + col) * nfx, *Y = sY + q * ncell, *Z = sZ + q * ncell;
-        auto fx = [&](int g) -> double {
-            g = wave_xface(I, g);
-            return g < 0 ? 0.0 : X[g - gl];
-        };
-        auto fy = [&](int jj) {
-            jj = jj < 0 ? jj + L.ny : (jj >= L.ny ? jj - L.ny : jj);
-            return Y[il + bx * (jj + L.ny * k)];
-        };
-        auto fz = [&](int kk) {
-            kk = kk < 0 ? kk + L.nz : (kk >= L.nz ? kk - L.nz : kk);
-            return Z[il + bx * (j + L.ny * kk)];
-        };
-        r[q] = wave_rhs(I, i, j, k, fx, fy, fz);
+    for (int t = threadIdx.x; t < ncell; t += blockDim.x) {
+        const int il = t % bx, col = t / bx, j = col % L.ny, k = col / L.ny, i = x0 + il;
+        double r[5];
+        for (int q = 0; q < 5; ++q) {
+            const double *X = sX + (q * ncol + col) * nfx, *Y = sY + q * ncell, *Z = sZ + q * ncell;
+            auto fx = [&](int g) -> double {
+                g = wave_xface(I, g);
+                return g < 0 ? 0.0 : X[g - gl];
+            };
+            auto fy = [&](int jj) {
+                jj = jj < 0 ? jj + L.ny : (jj >= L.ny ? jj - L.ny : jj);
+                return Y[il + bx * (jj + L.ny * k)];
+            };
+            auto fz = [&](int kk) {
+                kk = kk < 0 ? kk + L.nz : (kk >= L.nz ? kk - L.nz : kk);
+                return Z[il + bx * (j + L.ny * kk)];
+            };
+            r[q] = wave_rhs(I, i, j, k, fx, fy, fz);
+        }
+        wave_finish(a, I, L.at(i + NG, j + NG, k + NG), wave_dst(a), src, r, a.dt[p]);
     }
-    wave_finish(a, I, L.at(i + NG, j + NG, k + NG), wave_dst(a), src, r, a.dt[p]);
 }
 
 // shared memory of wave_brick_kernel for a problem (the largest brick)
