@@ -834,7 +834,7 @@ def main():
                 peak64 = sms * 64 * mhz * 1e6
                 fp64_pipe = {"achieved": rate, "peak": peak64, "unit": "FP64 thread-instructions/s",
                              "frac": rate / peak64, "fp64_instr_per_cell": float(f[1]),
-                             "source": "profiles/fp64_instr_per_cell_192.txt (ncu, one launch at 192^3)"}
+                             "source": "profiles/fp64_instr_per_cell_192.txt (one-kernel ncu captures at 192^3)"}
 
     # end to end through the C ABI with host buffers (pinned)
     e2e = e2e_full = None
