@@ -242,6 +242,9 @@ sweep_kernel(SweepArgs<R> a) {
     unsigned det_carry = 0;  // x-sweep detector bits of the previous chunk's last face (cell fc)
     // y/z-sweep detector bits, position p <-> cell fc + p (MDCD_HYBRID)
     __shared__ unsigned char sDet[(DIR != 0 && CHAR == 0 && INTERP == I_MDCD_HYBRID) ? (C + 1) * NL : 1];
+    // periodic x-lines: faces 0 .. 4 of each line, kept from the first chunk
+    // for faces n .. n+4 (the same wrapped cells, so the same bits)
+    __shared__ R sWrapF[(DIR == 0 && CHAR == 0 && INTERP == I_MDCD_HYBRID) ? 25 * NL : 1];
     float def_w[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, def_t = 0.f;
     const int slot = DIR == 0 ? threadIdx.x : threadIdx.y;
     const int line = DIR == 0 ? threadIdx.y : threadIdx.x;
@@ -387,7 +390,15 @@ sweep_kernel(SweepArgs<R> a) {
             // centre and takes the other from the lane before it (lane 0: from
             // lane 31 of the previous chunk; in the first chunk it evaluates
             // both).  Same values as evaluating both centres per face.
-            if (line_ok) {  // uniform over the warp
+            if (line_ok && per && fc >= n) {
+                // the last chunk of a periodic line holds only faces n .. n+4
+                // (fc >= n: uniform over the block): copies of faces 0 .. 4
+                if (f < fe) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q)
+                        sF[q * NL * NF + G::template idx<NF>(line, slot + 5)] = sWrapF[(q * NL + line) * 5 + (f - n)];
+                }
+            } else if (line_ok) {  // uniform over the warp
                 // one variable's stencil at a time (its registers die with it);
                 // the rare WENO branch re-reads its stencil from shared memory
                 R UL[5], UR[5];
@@ -431,6 +442,10 @@ sweep_kernel(SweepArgs<R> a) {
                     const int s = G::template idx<NF>(line, slot + 5);
 #pragma unroll
                     for (int q = 0; q < 5; ++q) sF[q * NL * NF + s] = F[q];
+                    if (per && f < 5) {  // first chunk (fb = 0 on periodic lines)
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) sWrapF[(q * NL + line) * 5 + f] = F[q];
+                    }
                 }
             }
         } else if constexpr (DIR != 0 && CHAR == 0 && INTERP == I_MDCD_HYBRID) {
