@@ -223,6 +223,9 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
     double2 *const sUf = reinterpret_cast<double2 *>(srold + 5 * CH);  // [5][CH] z: U0
     float2 *const sDs = reinterpret_cast<float2 *>(sUf + 5 * CH);      // [5][CH] z: stage increment
     float2 *const sDef = sDs + 5 * CH;                                 // [6][5][NP] z: deferred W, T
+    // periodic x-lines: faces 0 .. 4 of each pair, kept from the first chunk
+    // for faces n .. n+4 (the same wrapped cells, so the same bits)
+    __shared__ float2 sWrapF[DIR == 0 ? 25 * NP : 1];
 
     if (a.done && *a.done) return;  // uniform over the grid
     const Layout &L = a.L;
@@ -374,7 +377,15 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
 
         // ---- face f = fc + slot of both lines: cell positions slot .. slot+5
         const int f = fc + slot;
-        if (line_ok && f < fe) {
+        if (DIR == 0 && per && fc >= n) {
+            // the last chunk of a periodic x-line holds only faces n .. n+4
+            // (fc >= n: uniform over the block): copies of faces 0 .. 4
+            if (line_ok && f < fe) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q)
+                    sF[q * NP * NF + G::template idx<NF>(pr, slot + 5)] = sWrapF[(q * NP + pr) * 5 + (f - n)];
+            }
+        } else if (line_ok && f < fe) {
             // one variable's stencil at a time (its registers die with it);
             // the rare WENO branch re-reads its stencil from shared memory
             float2 UL[5], UR[5];
@@ -436,6 +447,10 @@ __global__ void __launch_bounds__(256, pair_min_blocks<DIR>()) sweep_pair_kernel
                 riemann<DIR, float, RS>(a.sp, ULb, URb, Fb);
 #pragma unroll
                 for (int q = 0; q < 5; ++q) sF[q * NP * NF + s] = make_float2(Fa[q], Fb[q]);
+            }
+            if (DIR == 0 && per && f < 5) {  // first chunk (fb = 0 on periodic lines)
+#pragma unroll
+                for (int q = 0; q < 5; ++q) sWrapF[(q * NP + pr) * 5 + f] = sF[q * NP * NF + s];
             }
         }
         cp_async_wait<1>();  // this thread's old-RHS / FP64-state copies landed
