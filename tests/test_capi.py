@@ -43,14 +43,34 @@ def test_defaults_and_status_strings(lib):
     assert lib.ns3d_status_string(-5) == b"non-finite state"
 
 
-def _create(lib, **kw):
+def _create(lib, grid=(8, 8, 8, 0, 0, 0, 1, 1, 1), **kw):
     p = _lib.Params()
     lib.ns3d_params_default(C.byref(p))
     for k, v in kw.items():
         setattr(p, k, v)
-    g = _lib.Grid(8, 8, 8, 0, 0, 0, 1, 1, 1)
+    g = _lib.Grid(*grid)
     h = C.c_void_p()
     return lib.ns3d_create(C.byref(p), C.byref(g), C.byref(h)), h
+
+
+@pytest.mark.parametrize("grid,why", [
+    ((2, 8, 8, 0, 0, 0, 1, 1, 1), b"at least 3"),          # narrower than the WCNS stencil's ghost layers
+    ((8, 8, 0, 0, 0, 0, 1, 1, 1), b"at least 3"),          # empty
+    ((-4, 8, 8, 0, 0, 0, 1, 1, 1), b"at least 3"),
+    ((2048, 2048, 1024, 0, 0, 0, 1, 1, 1), b"too large"),  # beyond 2^31 cells
+    ((8, 8, 8, 0, 0, 0, 1, 0, 1), b"positive"),            # zero domain length
+])
+def test_bad_grids_rejected_before_device(lib, grid, why):
+    r, h = _create(lib, grid=grid)
+    assert r == -2 and not h.value
+    assert why in lib.ns3d_last_error(None)
+
+
+@pytest.mark.parametrize("field,value", [("gamma", 1.0), ("Ma", 0.0), ("Re", -1.0), ("Pr", 0.0)])
+def test_bad_physical_constants_rejected(lib, field, value):
+    r, h = _create(lib, **{field: value})
+    assert r == -2 and not h.value
+    assert b"physical" in lib.ns3d_last_error(None)
 
 
 def test_zero_interpolation_rejected_before_device(lib):
