@@ -1,9 +1,11 @@
 """Batched independent problems (ns3d_batch_* of the C ABI).
 
 Many small ns3d_wcns runs of uneven size -- e.g. quasi-1D shock tubes on
-Nx x 4 x 4 grids -- integrated to their own end times in one persistent
-launch.  Each problem follows time_advance's dt schedule with its own CFL
-time step (maincycle.cpp:18-56).
+Nx x 4 x 4 grids -- integrated to their own end times on one GPU, by the
+wavefront schedule (every active problem one step per round of launches) or
+one persistent cluster launch, whichever ``autotune`` measures faster; both
+give the same bits.  Each problem follows time_advance's dt schedule with its
+own CFL time step (maincycle.cpp:18-56).
 """
 from __future__ import annotations
 
