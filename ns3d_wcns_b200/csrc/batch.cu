@@ -72,6 +72,18 @@ __device__ __forceinline__ double *arr(const BatchArgs &a, const Inst &I, int q)
     return a.pool + I.base + (long)q * I.L.plane;
 }
 
+// Which stored x-face gives the flux of face g of a line in the half-node
+// difference: periodic x wraps (face nx is face 0: the same stencil cells);
+// otherwise a face beyond the domain takes the boundary face's flux at an
+// outflow side and zero elsewhere (-1), the reference's ghost faces.
+__device__ __forceinline__ int batch_xface(const Inst &I, int g) {
+    const int nx = I.L.nx;
+    if (I.periodic[0]) return g < 0 ? g + nx : (g > nx ? g - nx : g);
+    if (g < 0) return I.bc[0] == BC_OUTFLOW ? 0 : -1;
+    if (g > nx) return I.bc[1] == BC_OUTFLOW ? nx : -1;
+    return g;
+}
+
 // Face flux of x-face g (between interior cells g-1 and g; g in [0, nx]) /
 // y-face, z-face g (between interior g and g+1, periodic wrap) of line (j,k),
 // from the stored conserved state U
@@ -216,9 +228,8 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(BatchArgs a) {
                     double R[5];
                     for (int q = 0; q < 5; ++q) {
                         auto fx = [&](int g) -> double {
-                            if (g < 0) { if (I.bc[0] == BC_OUTFLOW) g = 0; else return 0.0; }
-                            if (g > L.nx) { if (I.bc[1] == BC_OUTFLOW) g = L.nx; else return 0.0; }
-                            return FX(q)[((long)k * L.ny + j) * (L.nx + 1) + g];
+                            g = batch_xface(I, g);
+                            return g < 0 ? 0.0 : FX(q)[((long)k * L.ny + j) * (L.nx + 1) + g];
                         };
                         // cell i uses faces i-3 .. i+2 (ghost-inclusive), x-face g = f - (NG - 1)
                         auto dh = [](double f0, double f1, double f2, double f3, double f4, double f5, double ih) {
@@ -442,14 +453,6 @@ __device__ __forceinline__ double wave_rhs(const Inst &I, int i, int j, int k, F
     return r;
 }
 
-// x-face index with the boundary rule: faces beyond the domain take the
-// boundary face's flux at an outflow side, zero otherwise (-1)
-__device__ __forceinline__ int wave_xface(const Inst &I, int g) {
-    if (g < 0) return I.bc[0] == BC_OUTFLOW ? 0 : -1;
-    if (g > I.L.nx) return I.bc[1] == BC_OUTFLOW ? I.L.nx : -1;
-    return g;
-}
-
 // the stage update of interior cell c from its RHS and runge_kutta_3's
 // c2p -> p2c round trip (range_kutta.cpp:53-91)
 __device__ __forceinline__ void wave_finish(const WaveArgs &a, const Inst &I, long c, int dst, int src,
@@ -483,7 +486,7 @@ __global__ void __launch_bounds__(256) wave_update_kernel(WaveArgs a) {
     for (int q = 0; q < 5; ++q) {
         const double *FX = warr(a, I, 15 + q), *FY = warr(a, I, 20 + q), *FZ = warr(a, I, 25 + q);
         auto fx = [&](int g) -> double {
-            g = wave_xface(I, g);
+            g = batch_xface(I, g);
             return g < 0 ? 0.0 : FX[((long)k * L.ny + j) * (L.nx + 1) + g];
         };
         auto fy = [&](int jj) {
@@ -518,7 +521,11 @@ __global__ void __launch_bounds__(256, 3) wave_brick_kernel(WaveArgs a) {
     const Layout &L = I.L;
     const int ncol = L.ny * L.nz, x0 = a.tile_off[blockIdx.x];
     const int bx = min(brick_width(L), L.nx - x0);
-    const int gl = max(0, x0 - 2), gh = min(L.nx, x0 + bx + 2), nfx = gh - gl + 1;
+    // x-faces x0-2 .. x0+bx+2; without periodic x those beyond the domain
+    // follow the boundary rule in the update instead
+    const bool px = I.periodic[0] != 0;
+    const int gl = px ? x0 - 2 : max(0, x0 - 2), gh = px ? x0 + bx + 2 : min(L.nx, x0 + bx + 2);
+    const int nfx = gh - gl + 1;
     const int ncell = bx * ncol;
     // [q][col][face] x-faces, then [q][cell] y- and z-faces (cell = i + bx (j + ny k))
     double *sX = sfl, *sY = sX + 5 * nfx * ncol, *sZ = sY + 5 * ncell;
@@ -530,7 +537,7 @@ __global__ void __launch_bounds__(256, 3) wave_brick_kernel(WaveArgs a) {
     double F[5];
     for (int t = threadIdx.x; t < nfx * ncol; t += blockDim.x) {
         const int g = gl + t % nfx, col = t / nfx;
-        face_flux<0, INTERP, RS>(b, I, Uc, g, col % L.ny + NG, col / L.ny + NG, F);
+        face_flux<0, INTERP, RS>(b, I, Uc, batch_xface(I, g), col % L.ny + NG, col / L.ny + NG, F);
         for (int q = 0; q < 5; ++q) sX[(q * ncol + col) * nfx + (g - gl)] = F[q];
     }
     for (int t = threadIdx.x; t < ncell; t += blockDim.x) {
@@ -547,8 +554,8 @@ __global__ void __launch_bounds__(256, 3) wave_brick_kernel(WaveArgs a) {
         for (int q = 0; q < 5; ++q) {
             const double *X = sX + (q * ncol + col) * nfx, *Y = sY + q * ncell, *Z = sZ + q * ncell;
             auto fx = [&](int g) -> double {
-                g = wave_xface(I, g);
-                return g < 0 ? 0.0 : X[g - gl];
+                if (!px) g = batch_xface(I, g);
+                return !px && g < 0 ? 0.0 : X[g - gl];
             };
             auto fy = [&](int jj) {
                 jj = jj < 0 ? jj + L.ny : (jj >= L.ny ? jj - L.ny : jj);
@@ -567,7 +574,7 @@ __global__ void __launch_bounds__(256, 3) wave_brick_kernel(WaveArgs a) {
 // shared memory of wave_brick_kernel for a problem (the largest brick)
 inline size_t brick_smem(const Layout &L) {
     const int bx = std::min(brick_width(L), L.nx), ncol = L.ny * L.nz;
-    return sizeof(double) * 5 * ((size_t)std::min(bx + 5, L.nx + 1) * ncol + 2 * (size_t)bx * ncol);
+    return sizeof(double) * 5 * ((size_t)(bx + 5) * ncol + 2 * (size_t)bx * ncol);
 }
 
 // Within a run only two kinds of ghost cell are read: the x ghosts of

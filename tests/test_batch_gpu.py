@@ -102,13 +102,16 @@ def test_autotune_picks_a_valid_config_and_keeps_the_state(gpu_lib):
         assert max(rel_linf(a, r) for a, r in zip(b.primitives(0), W)) <= 1e-10
 
 
-def test_wavefront_bricks_and_wide_cross_sections(gpu_lib):
+@pytest.mark.parametrize("xbc", [(1, 3), (4, 3), (0, 0), (2, 1)], ids=["wall_outflow", "inflow_outflow",
+                                                                       "periodic", "symmetry_wall"])
+def test_wavefront_bricks_and_wide_cross_sections(gpu_lib, xbc):
     """Cross-sections of up to 64 cells take the fused brick kernel, wider ones
-    the separate face and update kernels; both in one batch, with walls in x
-    (sign flips in the ghost fill) and a state that varies in y and z.  Every
-    problem equals the persistent schedule bit for bit and the oracle."""
+    the separate face and update kernels; both in one batch, with every x
+    boundary type (sign flips and constants in the ghost fill, wrapped faces)
+    and a state that varies in y and z.  Every problem equals the persistent
+    schedule bit for bit, ghost cells included, and the oracle."""
     P, _ = make_params(n=(8, 4, 4), Ma=1.0, Re=math.inf, cfl=0.5, dt_fixed=-1.0, interpolation=0, riemann=0,
-                       bcs=(1, 3, 0, 0, 0, 0))
+                       bcs=(xbc[0], xbc[1], 0, 0, 0, 0))
     shapes = [(30, 4, 4), (26, 8, 8), (22, 9, 9), (18, 3, 5), (40, 3, 3)]
     rng = np.random.default_rng(7)
     grids, states, t_end = [], [], []
