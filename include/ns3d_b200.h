@@ -256,7 +256,8 @@ int ns3d_adjoint_kinetic_energy(ns3d_handle *h, int nsteps, double dt, int check
  * keep the whole GPU busy (faces and update fused per brick of 256/(ny nz)
  * x-cells by the cross-section when ny nz <= 64); the host drops finished
  * problems every 16 steps.
- * Both give the same bits.  ns3d_batch_autotune times the wavefront and the
+ * Both give the same bits for the compiled-in WENO5 + Roe instantiation (other
+ * schemes agree to rounding).  ns3d_batch_autotune times the wavefront and the
  * persistent cluster size (1,2,4,8) x CTA width (128,256) x resident CTAs
  * per SM (1,2,3: the register budget of the kernel instantiation) choices
  * and keeps the fastest; config_out = {cluster (0: wavefront), width, CTAs

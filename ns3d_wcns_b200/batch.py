@@ -4,7 +4,8 @@ Many small ns3d_wcns runs of uneven size -- e.g. quasi-1D shock tubes on
 Nx x 4 x 4 grids -- integrated to their own end times on one GPU, by the
 wavefront schedule (every active problem one step per round of launches) or
 one persistent cluster launch, whichever ``autotune`` measures faster; both
-give the same bits.  Each problem follows time_advance's dt schedule with its
+give the same bits for the compiled-in WENO5 + Roe scheme and agree to
+rounding for the others.  Each problem follows time_advance's dt schedule with its
 own CFL time step (maincycle.cpp:18-56).
 """
 from __future__ import annotations
