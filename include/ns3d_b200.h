@@ -351,8 +351,9 @@ int ns3d_rk3_stage(ns3d_handle *h, int stage, double dt);
 /* ---------------------------------------- scratch-free CFL time step
  * No counterpart in the reference.  For host codes that cannot let a library
  * allocate device memory -- solvers that hand out every device byte from
- * their own pre-sized pool, and codes that capture their time loop into a
- * CUDA graph -- this computes what ns3d_compute_timestep computes
+ * their own pre-sized pool, where a stray allocation breaks their memory
+ * accounting or fails once the pool holds the GPU's memory -- this computes
+ * what ns3d_compute_timestep computes
  * (compute_timestep, timestep.cpp:5-23) without a handle and without calling
  * cudaMalloc, cudaFree or any allocating routine.
  *   d_fields  five caller-owned device arrays rho, u, v, w, p in the unpadded

@@ -3,9 +3,8 @@
 //
 // Some host codes cannot let a library call cudaMalloc: solvers that carve
 // every device byte out of their own pre-sized pool (a stray allocation breaks
-// their memory accounting, or fails once the pool has taken the GPU's memory),
-// and codes that record their time loop into a CUDA graph, where an
-// allocation in the middle of the loop is not allowed.  For them this entry
+// their memory accounting, or fails once the pool has taken the GPU's
+// memory).  For them this entry
 // point does the work of ns3d_compute_timestep without a handle: its only
 // scratch, the per-block partial minima of the reduction, is a fixed
 // file-scope device array that every GPU which loads the library keeps until

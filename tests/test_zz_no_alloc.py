@@ -1,8 +1,9 @@
 """The scratch-free CFL time step (ns3d_compute_timestep_noalloc).
 
 Callers that cannot let the library allocate device memory -- codes that own
-every device byte through their own pool, or that capture their time loop
-into a CUDA graph -- pass their own device arrays and a device result slot;
+every device byte through their own pre-sized pool, where a library's
+allocation breaks their accounting or fails -- pass their own device arrays
+and a device result slot;
 the entry point's only scratch is a fixed device array inside the library.
 This file is collected last so that a failure here comes after every other
 test has run.  Its result must equal ns3d_compute_timestep's on the same
