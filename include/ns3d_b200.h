@@ -122,9 +122,17 @@ int ns3d_set_interior_primitives(ns3d_handle *h, const double *const fields[5]);
  *   NS3D_INIT_SOD         initialize_sod_shock_tube (initialization.cpp:568-596)
  *   NS3D_INIT_UNIFORM     initialize_uniform_field  (initialization.cpp:598-617)
  *   NS3D_INIT_SINE_X      initialize_sine_x_field   (initialization.cpp:619-638)
+ *   NS3D_INIT_ISOTROPIC   init_isotropic_turbulence (isotropic_ini.cpp:16-193):
+ *                         the seed-123 std::mt19937_64 phases, the k0 = 8
+ *                         spectrum, its inverse transform scaled to the
+ *                         reference's energy; rho = 1, T = 1.  Allocates
+ *                         scratch (three complex fields); at most 2048 cells
+ *                         per axis.  Each call starts the generator afresh (the
+ *                         reference's first call in a process).
  * Cells an initialiser does not write keep their current values (the
  * Field3D::allocate defaults on a new handle). */
-enum { NS3D_INIT_RIEMANN_2D = 0, NS3D_INIT_SOD = 1, NS3D_INIT_UNIFORM = 2, NS3D_INIT_SINE_X = 3 };
+enum { NS3D_INIT_RIEMANN_2D = 0, NS3D_INIT_SOD = 1, NS3D_INIT_UNIFORM = 2, NS3D_INIT_SINE_X = 3,
+       NS3D_INIT_ISOTROPIC = 4 };
 int ns3d_initialize(ns3d_handle *h, int kind);
 
 /* Download one group (NS3D_PRIMITIVE/CONSERVED/RHS: 5 arrays; TEMPERATURE: 1)

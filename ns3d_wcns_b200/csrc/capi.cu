@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/ns3d_b200.h"
+#include "isotropic.cuh"
 #include "adjoint_api.cuh"
 #include "common.cuh"
 #include "schemes.cuh"
@@ -1340,7 +1341,7 @@ int ns3d_set_interior_primitives(ns3d_handle *h, const double *const fields[5]) 
 }
 
 int ns3d_initialize(ns3d_handle *h, int kind) {
-    if (!h || kind < NS3D_INIT_RIEMANN_2D || kind > NS3D_INIT_SINE_X) return NS3D_ERR_INVALID_ARG;
+    if (!h || kind < NS3D_INIT_RIEMANN_2D || kind > NS3D_INIT_ISOTROPIC) return NS3D_ERR_INVALID_ARG;
     h->prev_valid = false;  // the free state buffers are scratch here
     int r = set_device(h); if (r) return r;
     h->launches = 0;
@@ -1357,9 +1358,13 @@ int ns3d_initialize(ns3d_handle *h, int kind) {
         for (int q = 0; q < 5; ++q)
             CK(h, cudaMemcpyAsync(h->S[b][q], h->S[h->s0][q], L.plane * 8, cudaMemcpyDeviceToDevice, h->stream), "copy");
     }
-    init_kernel<<<cell_grid(L, true, 128), 128, 0, h->stream>>>(state_table(h, b), L, kind, h->ph.dx, h->ph.dy,
-                                                                 h->G.Lx);
-    h->launches += 1;
+    if (kind == NS3D_INIT_ISOTROPIC) {
+        if ((r = isotropic_fill(state_table(h, b), L, h->ph.Rgas, h->stream, h->err))) return r;
+    } else {
+        init_kernel<<<cell_grid(L, true, 128), 128, 0, h->stream>>>(state_table(h, b), L, kind, h->ph.dx, h->ph.dy,
+                                                                     h->G.Lx);
+        h->launches += 1;
+    }
     CK(h, cudaGetLastError(), "initialiser");
     // apply_boundary + primitiveToConserved (main.cpp:98-99)
     if ((r = finish_upload(h, b, true))) return r;

@@ -110,11 +110,12 @@ class Solver:
                 raise ValueError("expected interior-sized arrays")
         self._check(self.lib.ns3d_set_interior_primitives(self.h, self._ptrs(arrs)))
 
-    INIT_KINDS = {"riemann_2d": 0, "sod": 1, "uniform": 2, "sine_x": 3}
+    INIT_KINDS = {"riemann_2d": 0, "sod": 1, "uniform": 2, "sine_x": 3, "isotropic": 4}
 
     def initialize(self, kind: str) -> None:
         """One of the reference's built-in initialisers on the device, then the
-        ghost fill (main.cpp:85-99): riemann_2d, sod, uniform or sine_x."""
+        ghost fill (main.cpp:85-99): riemann_2d, sod, uniform, sine_x or
+        isotropic (init_isotropic_turbulence, isotropic_ini.cpp:131-193)."""
         self._check(self.lib.ns3d_initialize(self.h, self.INIT_KINDS[kind]))
 
     def download(self, what: int) -> np.ndarray:

@@ -211,8 +211,9 @@ class RefSolver(_Base):
         return out
 
     def initialize(self, kind: str) -> None:
-        """initialize_riemann_2d / _sod_shock_tube / _uniform_field / _sine_x_field + ghost fill."""
-        r = self.lib.ref_initialize({"riemann_2d": 0, "sod": 1, "uniform": 2, "sine_x": 3}[kind])
+        """initialize_riemann_2d / _sod_shock_tube / _uniform_field / _sine_x_field /
+        init_isotropic_turbulence + ghost fill."""
+        r = self.lib.ref_initialize({"riemann_2d": 0, "sod": 1, "uniform": 2, "sine_x": 3, "isotropic": 4}[kind])
         if r != 0:
             raise RuntimeError("ref_initialize failed")
 
@@ -267,3 +268,15 @@ class Kernels:
         out = np.zeros(5)
         self._r(int(solver), _ptr(a), _ptr(b), int(direction), float(gamma), _ptr(out))
         return out
+
+
+def ref_isotropic(nx: int, ny: int, nz: int):
+    """The reference's generate_full_turbulence (isotropic_ini.cpp:26-126) on an
+    nx x ny x nz grid, from its generator's seed, as (u, v, w) arrays
+    [nz, ny, nx] of the interior."""
+    lib = C.CDLL(REF_LIB)
+    lib.ref_isotropic_field.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
+    out = [np.zeros(nx * ny * nz) for _ in range(3)]
+    lib.ref_isotropic_field(nx, ny, nz, *[_ptr(a) for a in out])
+    # reference order (i*ny + j)*nz + k -> [k][j][i]
+    return tuple(np.ascontiguousarray(a.reshape(nx, ny, nz).transpose(2, 1, 0)) for a in out)

@@ -22,6 +22,17 @@
 
 #include "field_structures.h"
 #include "ns3d_func.h"
+#include <thread>
+
+// Runs fn on a new thread.  The reference's isotropic initialiser draws from a
+// thread_local std::mt19937_64 seeded on first use in a thread
+// (isotropic_ini.cpp:16-20), so on a fresh thread every call starts from the
+// seed, as the reference's first call in a process does.
+template <class F>
+static void on_fresh_thread(F fn) {
+    std::thread t(fn);
+    t.join();
+}
 
 // The reference's post-processing writers live in files that need FFTW/HDF5;
 // the oracle build leaves those files out and supplies no-op definitions.
@@ -180,6 +191,7 @@ int ref_initialize(int kind) {
         case 1: initialize_sod_shock_tube(S->F, S->G, S->P); break;
         case 2: initialize_uniform_field(S->F, S->G, S->P); break;
         case 3: initialize_sine_x_field(S->F, S->G, S->P); break;
+        case 4: on_fresh_thread([] { init_isotropic_turbulence(S->F, S->G, S->C, S->P); }); break;
         default: return -1;
     }
     apply_boundary(S->F, S->G, S->C, S->P);
@@ -247,6 +259,15 @@ void ref_riemann(int solver, const double *UL, const double *UR, int dir, double
         case 5: AUSM_Riemann_solver(out, L, R, nx, ny, nz, gamma); break;
     }
     for (int i = 0; i < 5; ++i) F[i] = out[i];
+}
+
+// generate_full_turbulence (isotropic_ini.cpp:26-126): the velocity field in the
+// reference's order, index (i*ny + j)*nz + k, from the generator's seed.
+int ref_isotropic_field(int nx, int ny, int nz, double *u, double *v, double *w) {
+    std::vector<double> U, V, W;
+    on_fresh_thread([&] { generate_full_turbulence(nx, ny, nz, U, V, W); });
+    for (size_t id = 0; id < U.size(); ++id) { u[id] = U[id]; v[id] = V[id]; w[id] = W[id]; }
+    return 0;
 }
 
 }  // extern "C"
